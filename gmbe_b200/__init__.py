@@ -1,0 +1,248 @@
+"""Python binding of the B200 maximal biclique enumeration engine.
+
+Thin ctypes layer over the C ABI in ``include/mbe.h`` (``libgmbe.so``, built
+in-tree by ``gmbe_b200/csrc/Makefile``).  The reference's own surface is C++
+(``CSRBiGraph``, ``IterFinderGpu6``; see ``include/mbe_finder.h``); this module
+exists for tests, the benchmark and scripting.  There is no CPU fallback: if
+the shared library is missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgmbe.so")
+CLI_PATH = os.path.join(_HERE, "MBE_GPU")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `make -C gmbe_b200/csrc` "
+        "(or __graft_entry__.build()); the engine has no CPU fallback")
+_lib = C.CDLL(LIB_PATH)
+
+MBE_OK = 0
+ERRORS = {
+    -1: "MBE_ERR_INVALID", -2: "MBE_ERR_IO", -3: "MBE_ERR_FORMAT", -4: "MBE_ERR_CUDA",
+    -5: "MBE_ERR_NOMEM", -6: "MBE_ERR_TIMEOUT", -7: "MBE_ERR_QUEUE_FULL",
+    -8: "MBE_ERR_CAPACITY", -9: "MBE_ERR_ADMISSION", -10: "MBE_ERR_CANCELLED",
+    -11: "MBE_ERR_NOT_FOUND", -12: "MBE_ERR_AGAIN",
+}
+
+
+class MBEError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+        self.name = ERRORS.get(code, str(code))
+
+
+class Opts(C.Structure):
+    _fields_ = [("uvtrans", C.c_int32), ("order", C.c_int32), ("fast_mode", C.c_int32),
+                ("device", C.c_int32)]
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("U_size", C.c_int32), ("V_size", C.c_int32), ("edge_size", C.c_int64),
+                ("U_degree", C.c_int32), ("V_degree", C.c_int32), ("U_2degree", C.c_int32),
+                ("V_2degree", C.c_int32), ("swapped", C.c_int32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("bound_height", C.c_int32), ("bound_size", C.c_int32), ("prune", C.c_int32),
+                ("blocks", C.c_int32), ("queue_capacity", C.c_int32),
+                ("bitmap_max_l", C.c_int32), ("wait_limit_ns", C.c_int64),
+                ("sm_timing", C.c_int32), ("root_begin", C.c_int32), ("root_end", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class Result(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("set_hash", C.c_uint64), ("non_maximal", C.c_uint64),
+                ("tasks_split", C.c_uint64), ("enum_seconds", C.c_double),
+                ("kernel_ms", C.c_float), ("status", C.c_int32),
+                ("sm_exit_max_ms", C.c_double), ("sm_exit_min_ms", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class GenSpec(C.Structure):
+    _fields_ = [("nU", C.c_int64), ("nV", C.c_int64), ("n_edges", C.c_int64),
+                ("gamma_u", C.c_double), ("gamma_v", C.c_double),
+                ("max_deg_u", C.c_int64), ("max_deg_v", C.c_int64), ("seed", C.c_uint64),
+                ("n_blocks", C.c_int32), ("block_u", C.c_int32), ("block_v", C.c_int32),
+                ("reserved", C.c_int32), ("block_p", C.c_double), ("pair_p_max", C.c_double)]
+
+
+_P32 = C.POINTER(C.c_int32)
+_sig = {
+    "mbe_params_default": (None, [C.POINTER(Params)]),
+    "mbe_opts_default": (None, [C.POINTER(Opts)]),
+    "mbe_graph_from_adj": (C.c_int, [C.c_char_p, C.POINTER(Opts), C.POINTER(C.c_void_p)]),
+    "mbe_graph_from_csr": (C.c_int, [_P32, _P32, C.c_int32, C.c_int32, C.c_int64,
+                                     C.POINTER(Opts), C.POINTER(C.c_void_p)]),
+    "mbe_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(GraphInfo)]),
+    "mbe_graph_free": (C.c_int, [C.c_void_p]),
+    "mbe_enumerate": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]),
+    "mbe_last_error_string": (C.c_char_p, []),
+    "mbe_gen_chung_lu": (C.c_int, [C.POINTER(GenSpec), C.POINTER(_P32), C.POINTER(_P32),
+                                   _P32, _P32, C.POINTER(C.c_int64)]),
+    "mbe_gen_batch_spec": (C.c_int, [C.c_uint64, C.POINTER(GenSpec)]),
+    "mbe_write_adj": (C.c_int, [C.c_char_p, _P32, _P32, C.c_int32]),
+    "mbe_read_adj": (C.c_int, [C.c_char_p, C.POINTER(_P32), C.POINTER(_P32), _P32, _P32,
+                               C.POINTER(C.c_int64)]),
+    "mbe_free": (None, [C.c_void_p]),
+}
+for _name, (_res, _args) in _sig.items():
+    _f = getattr(_lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def last_error() -> str:
+    s = _lib.mbe_last_error_string()
+    return s.decode() if s else ""
+
+
+def _check(rc: int):
+    if rc != MBE_OK:
+        raise MBEError(rc, last_error())
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P32)
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    _lib.mbe_params_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise TypeError(f"unknown parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+def make_opts(uvtrans=0, order=1, fast_mode=1, device=0) -> Opts:
+    return Opts(uvtrans, order, fast_mode, device)
+
+
+class Graph:
+    """A bipartite graph resident on the GPU (reference CSRBiGraph after
+    Read + CopyToGpu).  V rows are .adj lines, entries U ids."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def from_csr(cls, row_off, col, nU: int = 0, uvtrans=0, order=1, fast_mode=1, device=0):
+        ro, co = _i32(row_off), _i32(col)
+        h = C.c_void_p()
+        opts = make_opts(uvtrans, order, fast_mode, device)
+        _check(_lib.mbe_graph_from_csr(_ptr(ro), _ptr(co), len(ro) - 1, int(nU), len(co),
+                                       C.byref(opts), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_adj(cls, path: str, uvtrans=0, order=1, fast_mode=1, device=0):
+        h = C.c_void_p()
+        opts = make_opts(uvtrans, order, fast_mode, device)
+        _check(_lib.mbe_graph_from_adj(os.fsencode(path), C.byref(opts), C.byref(h)))
+        return cls(h.value)
+
+    def info(self) -> GraphInfo:
+        i = GraphInfo()
+        _check(_lib.mbe_graph_get_info(self._h, C.byref(i)))
+        return i
+
+    def enumerate(self, **params) -> Result:
+        p = default_params(**params)
+        r = Result()
+        _check(_lib.mbe_enumerate(self._h, C.byref(p), C.byref(r)))
+        return r
+
+    def free(self):
+        if self._h and self._h.value:
+            _lib.mbe_graph_free(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Synthetic inputs.
+
+@dataclass
+class BipartiteCSR:
+    row_off: np.ndarray  # int32 [nV+1]
+    col: np.ndarray      # int32 [nE]
+    nU: int
+
+    @property
+    def nV(self) -> int:
+        return len(self.row_off) - 1
+
+    @property
+    def nE(self) -> int:
+        return len(self.col)
+
+
+def generate(spec: GenSpec) -> BipartiteCSR:
+    ro, co = _P32(), _P32()
+    nV, nU, nE = C.c_int32(), C.c_int32(), C.c_int64()
+    _check(_lib.mbe_gen_chung_lu(C.byref(spec), C.byref(ro), C.byref(co), C.byref(nV),
+                                 C.byref(nU), C.byref(nE)))
+    try:
+        r = np.ctypeslib.as_array(ro, (nV.value + 1,)).copy()
+        c = (np.ctypeslib.as_array(co, (nE.value,)).copy() if nE.value
+             else np.zeros(0, np.int32))
+    finally:
+        _lib.mbe_free(ro)
+        _lib.mbe_free(co)
+    return BipartiteCSR(r, c, nU.value)
+
+
+def batch_spec(seed: int) -> GenSpec:
+    s = GenSpec()
+    _check(_lib.mbe_gen_batch_spec(C.c_uint64(seed), C.byref(s)))
+    return s
+
+
+def write_adj(path: str, g: BipartiteCSR):
+    ro, co = _i32(g.row_off), _i32(g.col)
+    _check(_lib.mbe_write_adj(os.fsencode(path), _ptr(ro), _ptr(co), g.nV))
+
+
+def read_adj(path: str) -> BipartiteCSR:
+    ro, co = _P32(), _P32()
+    nV, nU, nE = C.c_int32(), C.c_int32(), C.c_int64()
+    _check(_lib.mbe_read_adj(os.fsencode(path), C.byref(ro), C.byref(co), C.byref(nV),
+                             C.byref(nU), C.byref(nE)))
+    try:
+        r = np.ctypeslib.as_array(ro, (nV.value + 1,)).copy()
+        c = (np.ctypeslib.as_array(co, (nE.value,)).copy() if nE.value
+             else np.zeros(0, np.int32))
+    finally:
+        _lib.mbe_free(ro)
+        _lib.mbe_free(co)
+    return BipartiteCSR(r, c, nU.value)
+
+
+from .configs import CONFIGS, DESCRIPTIONS, batch_graph, config_graph  # noqa: E402,F401

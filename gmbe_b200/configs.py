@@ -1,0 +1,56 @@
+"""The benchmark workloads as seeded generator specs.
+
+Each configuration is a Chung-Lu bipartite graph (see ``mbe_gen_chung_lu`` in
+include/mbe.h) with the shape the workload names.  All of them cap the
+probability of any single (u, v) pair at 0.1: with hub weights whose product
+exceeds the edge count, plain Chung-Lu saturates a block of hubs to a
+near-complete bipartite graph, and the few missing edges of such a block give
+2^k maximal bicliques for k hubs (measured: the top roots of the uncapped
+medium graph hold 1, 2, 4, ..., 128 bicliques each), which no enumerator can
+finish.  The cap keeps every marginal named by the workload (sizes, edge
+count, exponents, degree caps as expected-degree caps) and removes only that
+saturation.
+"""
+from __future__ import annotations
+
+from . import GenSpec, batch_spec, generate
+
+PAIR_P_MAX = 0.1
+
+
+def _spec(nU, nV, nE, gu, gv, mu, mv, seed, n_blocks=0, bu=0, bv=0, bp=0.0):
+    return GenSpec(nU=nU, nV=nV, n_edges=nE, gamma_u=gu, gamma_v=gv, max_deg_u=mu,
+                   max_deg_v=mv, seed=seed, n_blocks=n_blocks, block_u=bu, block_v=bv,
+                   reserved=0, block_p=bp, pair_p_max=PAIR_P_MAX)
+
+
+CONFIGS = {
+    # small: 2,000 x 3,000, ~20,000 edges, exponent 2.1 both sides, degree cap 200
+    "small": lambda: _spec(2000, 3000, 20000, 2.1, 2.1, 200, 200, 1),
+    # medium skewed: 100,000 x 400,000, ~2,000,000 edges, exponents 2.0 / 2.4,
+    # degree cap 5,000, plus 64 planted 24 x 24 blocks at edge probability 0.7
+    "medium": lambda: _spec(100000, 400000, 2000000, 2.0, 2.4, 5000, 5000, 2, 64, 24, 24, 0.7),
+    # large: 2,000,000 x 8,000,000, ~60,000,000 edges, exponents 2.1 / 2.2, cap 50,000
+    "large": lambda: _spec(2000000, 8000000, 60000000, 2.1, 2.2, 50000, 50000, 3),
+    # serving mix, medium requests: 20,000 x 80,000, ~300,000 edges, exponent 2.1
+    "serve_medium": lambda: _spec(20000, 80000, 300000, 2.1, 2.1, 2000, 2000, 7),
+}
+
+# Workload names as the benchmark reports them.
+DESCRIPTIONS = {
+    "small": "MBE 2k x 3k Chung-Lu (gamma 2.1/2.1, cap 200, seed 1, ~20k edges)",
+    "medium": ("MBE 100k x 400k Chung-Lu (gamma 2.0/2.4, cap 5000, seed 2, ~2M edges) "
+               "+ 64 planted 24x24 blocks p=0.7"),
+    "large": "MBE 2M x 8M Chung-Lu (gamma 2.1/2.2, cap 50000, seed 3, ~60M edges)",
+    "serve_medium": "MBE 20k x 80k Chung-Lu (gamma 2.1, cap 2000, ~300k edges)",
+}
+
+
+def config_graph(name: str):
+    """Generates the named workload graph (host CSR, .adj-shaped)."""
+    return generate(CONFIGS[name]())
+
+
+def batch_graph(seed: int):
+    """One graph of the batched workload (seeds 1000..5095)."""
+    return generate(batch_spec(seed))

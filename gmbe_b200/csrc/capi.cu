@@ -1,0 +1,391 @@
+// extern "C" layer: graph lifetime, device upload and the enumeration launch.
+// See include/mbe.h for the contract and the reference interfaces replaced.
+#include <cuda_runtime.h>
+#include <sys/time.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "enum_launch.h"
+#include "internal.h"
+
+using namespace gmbe;
+
+struct mbe_graph {
+  HostGraph h;
+  mbe_opts opts;
+  int device = 0;
+  int32_t* d_row_off = nullptr;
+  int32_t* d_col = nullptr;
+  int32_t* d_rev_off = nullptr;
+  int32_t* d_rev_col = nullptr;
+  uint64_t* d_ukey = nullptr;
+  uint64_t* d_vkey = nullptr;
+  // Cached engine workspace (grown on demand, reused across enumerations).
+  int32_t* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  EnumCtl* d_ctl = nullptr;
+  Task* d_q_tasks = nullptr;
+  unsigned long long* d_q_seq = nullptr;
+  int32_t q_cap = 0;
+  unsigned long long* d_exit = nullptr;
+  int32_t exit_cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Capacities derived from the graph (max over roots).
+  int32_t capS = 0, capL = 0;
+};
+
+namespace {
+
+double now_s() {
+  struct timeval tv;
+  gettimeofday(&tv, nullptr);
+  return (double)tv.tv_sec + (double)tv.tv_usec * 1e-6;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return set_error(MBE_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                                  \
+  do {                                                            \
+    cudaError_t _e = (call);                                      \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call);           \
+  } while (0)
+
+inline uint64_t fmix64_h(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+void free_device(mbe_graph* g) {
+  cudaFree(g->d_row_off);
+  cudaFree(g->d_col);
+  cudaFree(g->d_rev_off);
+  cudaFree(g->d_rev_col);
+  cudaFree(g->d_ukey);
+  cudaFree(g->d_vkey);
+  cudaFree(g->d_scratch);
+  cudaFree(g->d_ctl);
+  cudaFree(g->d_q_tasks);
+  cudaFree(g->d_q_seq);
+  cudaFree(g->d_exit);
+  if (g->ev0) cudaEventDestroy(g->ev0);
+  if (g->ev1) cudaEventDestroy(g->ev1);
+  g->d_row_off = g->d_col = g->d_rev_off = g->d_rev_col = nullptr;
+  g->d_ukey = g->d_vkey = nullptr;
+  g->d_scratch = nullptr;
+  g->d_ctl = nullptr;
+  g->d_q_tasks = nullptr;
+  g->d_q_seq = nullptr;
+  g->d_exit = nullptr;
+  g->ev0 = g->ev1 = nullptr;
+}
+
+template <typename T>
+int upload(T** dst, const std::vector<T>& src) {
+  size_t n = std::max<size_t>(src.size(), 1);
+  CK(cudaMalloc((void**)dst, n * sizeof(T)));
+  if (!src.empty()) CK(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return MBE_OK;
+}
+
+int upload_graph(mbe_graph* g) {
+  CK(cudaSetDevice(g->device));
+  const HostGraph& h = g->h;
+  int rc;
+  if ((rc = upload(&g->d_row_off, h.row_off))) return rc;
+  if ((rc = upload(&g->d_col, h.col))) return rc;
+  if ((rc = upload(&g->d_rev_off, h.rev_off))) return rc;
+  if ((rc = upload(&g->d_rev_col, h.rev_col))) return rc;
+  // Hash keys in original ids and original sides (see include/mbe.h).
+  std::vector<uint64_t> uk(h.U_size), vk(h.V_size);
+  for (int32_t u = 0; u < h.U_size; ++u)
+    uk[u] = fmix64_h((uint64_t)h.u_orig[u] * 2u + (h.swapped ? 1u : 0u));
+  for (int32_t v = 0; v < h.V_size; ++v)
+    vk[v] = fmix64_h((uint64_t)h.v_orig[v] * 2u + (h.swapped ? 0u : 1u));
+  if ((rc = upload(&g->d_ukey, uk))) return rc;
+  if ((rc = upload(&g->d_vkey, vk))) return rc;
+  // Capacities: max over roots of |N(v)| and of sum_{u in N(v)} d(u).
+  int64_t capS = 0;
+  int32_t capL = 0;
+  for (int32_t v = 0; v < h.V_size; ++v) {
+    int64_t s = 0;
+    for (int32_t i = h.row_off[v]; i < h.row_off[v + 1]; ++i) {
+      int32_t u = h.col[i];
+      s += h.rev_off[u + 1] - h.rev_off[u];
+    }
+    capS = std::max(capS, s);
+    capL = std::max(capL, h.row_off[v + 1] - h.row_off[v]);
+  }
+  if (capS > INT32_MAX / 2) return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
+  g->capS = (int32_t)std::max<int64_t>(capS, 1);
+  g->capL = std::max(capL, 1);
+  CK(cudaEventCreate(&g->ev0));
+  CK(cudaEventCreate(&g->ev1));
+  return MBE_OK;
+}
+
+int finish_graph(mbe_graph* g, const mbe_opts& o, mbe_graph** out) {
+  int rc = upload_graph(g);
+  if (rc) {
+    free_device(g);
+    delete g;
+    return rc;
+  }
+  *out = g;
+  return MBE_OK;
+}
+
+}  // namespace
+
+namespace gmbe {
+
+ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) {
+  ScratchLayout s;
+  memset(&s, 0, sizeof(s));
+  s.capC = capC;
+  s.capL = capL;
+  s.capS = capS;
+  s.kmax = kKMax;
+  int64_t off = 0;
+  auto take = [&](int64_t words) {
+    int64_t o = off;
+    off += (words + 7) & ~int64_t(7);  // 32-byte aligned slices
+    return o;
+  };
+  const int64_t C = capC, Lc = capL, S = capS, T2 = 32 * kKMax;
+  s.map = take(nV);
+  s.touched = take(C);
+  s.cv = take(C);
+  s.ncnt = take(C);
+  s.bound = take(C);
+  s.coff = take(C + 1);
+  s.fill = take(C);
+  s.sidx = take(C);
+  s.lv = take(Lc);
+  s.llevel = take(Lc);
+  s.lp = take(Lc);
+  s.aoff = take(Lc + 1);
+  s.stack = take(Lc + 2);
+  s.lsize = take(Lc + 2);
+  s.aadj = take(S);
+  s.cadj = take(S);
+  s.masks = take((int64_t)kKMax * C);
+  s.sub_v = take(2 * C);
+  s.bound2 = take(C);
+  s.lkey = take(2 * T2);
+  s.lmask = take((T2 + 2) * kKMax);
+  s.cursor2 = take(T2 + 2);
+  s.sr2 = take(2 * (T2 + 2));
+  s.nr2 = take(T2 + 2);
+  s.words_per_warp = off;
+  return s;
+}
+
+}  // namespace gmbe
+
+extern "C" {
+
+void mbe_params_default(mbe_params* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->bound_height = 20;
+  p->bound_size = 1500;
+  p->prune = 1;
+}
+
+void mbe_opts_default(mbe_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->order = 1;  // reference Option() default (src/BiGraph.h:17-21)
+}
+
+const char* mbe_last_error_string(void);
+
+int mbe_graph_from_csr(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t nU,
+                       int64_t nE, const mbe_opts* opts, mbe_graph** out) {
+  clear_error();
+  if (!out) return set_error(MBE_ERR_INVALID, "null output handle");
+  *out = nullptr;
+  mbe_opts o;
+  if (opts) o = *opts;
+  else mbe_opts_default(&o);
+  mbe_graph* g = new mbe_graph();
+  g->opts = o;
+  g->device = o.device;
+  int rc = build_host_graph(row_off, col, nV, nU, nE, o, &g->h);
+  if (rc) {
+    delete g;
+    return rc;
+  }
+  return finish_graph(g, o, out);
+}
+
+int mbe_graph_from_adj(const char* path, const mbe_opts* opts, mbe_graph** out) {
+  clear_error();
+  if (!path || !out) return set_error(MBE_ERR_INVALID, "null argument");
+  *out = nullptr;
+  std::vector<int32_t> ro, co;
+  int32_t nU = 0;
+  int rc = read_adj_file(path, &ro, &co, &nU);
+  if (rc) return rc;
+  return mbe_graph_from_csr(ro.data(), co.data(), (int32_t)ro.size() - 1, nU, (int64_t)co.size(),
+                            opts, out);
+}
+
+int mbe_graph_get_info(const mbe_graph* g, mbe_graph_info* info) {
+  clear_error();
+  if (!g || !info) return set_error(MBE_ERR_INVALID, "null argument");
+  info->U_size = g->h.U_size;
+  info->V_size = g->h.V_size;
+  info->edge_size = g->h.edge_size;
+  info->U_degree = g->h.U_degree;
+  info->V_degree = g->h.V_degree;
+  info->U_2degree = g->h.U_2degree;
+  info->V_2degree = g->h.V_2degree;
+  info->swapped = g->h.swapped;
+  return MBE_OK;
+}
+
+int mbe_graph_free(mbe_graph* g) {
+  clear_error();
+  if (!g) return MBE_OK;
+  cudaSetDevice(g->device);
+  free_device(g);
+  delete g;
+  return MBE_OK;
+}
+
+int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
+  clear_error();
+  if (!g || !out) return set_error(MBE_ERR_INVALID, "null argument");
+  memset(out, 0, sizeof(*out));
+  mbe_params prm;
+  if (params) prm = *params;
+  else mbe_params_default(&prm);
+  const double t0 = now_s();  // reference exe_time_ starts at Execute() (src/IterFinderGpu.cu:1096)
+  CK(cudaSetDevice(g->device));
+  const HostGraph& h = g->h;
+  int32_t rb = prm.root_begin, re = prm.root_end;
+  if (rb == 0 && re == 0) re = h.V_size;
+  if (rb < 0 || re > h.V_size || rb > re)
+    return set_error(MBE_ERR_INVALID, "root range [%d,%d) outside [0,%d)", rb, re, h.V_size);
+  int t2 = prm.bitmap_max_l;
+  if (t2 == 0) t2 = 32 * kKMax;
+  if (t2 < 0) t2 = 1;
+  if (t2 > 32 * kKMax) return set_error(MBE_ERR_INVALID, "bitmap_max_l > %d", 32 * kKMax);
+
+  // ---- launch shape and workspace ----
+  int dev_sms = 0;
+  CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
+  if (occ < 1) return set_error(MBE_ERR_CUDA, "enumeration kernel cannot be resident");
+  int blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * occ) : dev_sms * occ;
+  const int warps = blocks * kEnumWarps;
+  int32_t capC = std::max<int32_t>(1, std::min<int32_t>(h.V_size, g->capS));
+  ScratchLayout sl = make_layout(h.V_size, capC, g->capL, g->capS);
+  size_t need = (size_t)sl.words_per_warp * (size_t)warps * sizeof(int32_t);
+  if (need > g->scratch_bytes) {
+    cudaFree(g->d_scratch);
+    g->d_scratch = nullptr;
+    g->scratch_bytes = 0;
+    cudaError_t e = cudaMalloc((void**)&g->d_scratch, need);
+    if (e != cudaSuccess)
+      return set_error(MBE_ERR_NOMEM, "scratch of %.2f GB: %s", need / 1e9, cudaGetErrorString(e));
+    g->scratch_bytes = need;
+    CK(cudaMemset(g->d_scratch, 0, need));  // the dense count maps start (and end) at zero
+  }
+  int32_t qcap = prm.queue_capacity > 0
+                     ? prm.queue_capacity
+                     : (int32_t)std::min<int64_t>(1 << 22, std::max<int64_t>(1 << 16, 8LL * h.V_size));
+  if (qcap != g->q_cap) {
+    cudaFree(g->d_q_tasks);
+    cudaFree(g->d_q_seq);
+    g->d_q_tasks = nullptr;
+    g->d_q_seq = nullptr;
+    CK(cudaMalloc((void**)&g->d_q_tasks, sizeof(Task) * (size_t)qcap));
+    CK(cudaMalloc((void**)&g->d_q_seq, sizeof(unsigned long long) * (size_t)qcap));
+    g->q_cap = qcap;
+  }
+  if (!g->d_ctl) CK(cudaMalloc((void**)&g->d_ctl, sizeof(EnumCtl)));
+  if (blocks > g->exit_cap) {
+    cudaFree(g->d_exit);
+    CK(cudaMalloc((void**)&g->d_exit, sizeof(unsigned long long) * (size_t)blocks));
+    g->exit_cap = blocks;
+  }
+  CK(cudaMemsetAsync(g->d_ctl, 0, sizeof(EnumCtl)));
+  CK(cudaMemsetAsync(g->d_q_seq, 0, sizeof(unsigned long long) * (size_t)qcap));
+
+  DevGraph dg;
+  dg.nV = h.V_size;
+  dg.nU = h.U_size;
+  dg.nE = h.edge_size;
+  dg.row_off = g->d_row_off;
+  dg.col = g->d_col;
+  dg.rev_off = g->d_rev_off;
+  dg.rev_col = g->d_rev_col;
+  dg.ukey = g->d_ukey;
+  dg.vkey = g->d_vkey;
+  dg.swapped = h.swapped;
+  dg.root_begin = rb;
+  dg.root_end = re;
+  EnumParams ep;
+  memset(&ep, 0, sizeof(ep));
+  ep.bound_height = prm.bound_height;
+  ep.bound_size = prm.bound_size;
+  ep.prune = prm.prune;
+  ep.queue_cap = qcap;
+  ep.slot_spin_limit = 20000000;  // x ~64 ns sleeps: a claimed slot is written within microseconds
+  ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
+  ep.record_exit = prm.sm_timing ? 1 : 0;
+  ep.tier2_max_l = t2;
+
+  CK(cudaEventRecord(g->ev0));
+  mbe_enum_kernel<<<blocks, kEnumThreads>>>(dg, ep, sl, g->d_ctl, g->d_q_tasks, g->d_q_seq,
+                                            g->d_scratch, g->d_exit);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(g->ev1));
+  EnumCtl ctl;
+  CK(cudaMemcpy(&ctl, g->d_ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+  out->count = ctl.count;
+  out->set_hash = ctl.hash;
+  out->non_maximal = ctl.non_maximal;
+  out->tasks_split = ctl.tasks_split;
+  out->kernel_ms = ms;
+  out->status = ctl.status;
+  if (prm.sm_timing) {
+    std::vector<unsigned long long> ex(blocks);
+    CK(cudaMemcpy(ex.data(), g->d_exit, sizeof(unsigned long long) * blocks, cudaMemcpyDeviceToHost));
+    auto mm = std::minmax_element(ex.begin(), ex.end());
+    out->sm_exit_min_ms = *mm.first / 1e6;
+    out->sm_exit_max_ms = *mm.second / 1e6;
+  }
+  out->enum_seconds = now_s() - t0;
+  if (ctl.status != 0) {
+    // An aborted run leaves count maps dirty: clear them for the next call.
+    cudaMemset(g->d_scratch, 0, g->scratch_bytes);
+    switch (ctl.status) {
+      case kStTimeout:
+        return set_error(MBE_ERR_TIMEOUT, "device wait limit reached (idle %llu ns)", ctl.err_info);
+      case kStQueue:
+        return set_error(MBE_ERR_TIMEOUT, "split-queue slot %llu was never written", ctl.err_info);
+      case kStCapacity:
+        return set_error(MBE_ERR_CAPACITY, "scratch capacity exceeded (info 0x%llx)", ctl.err_info);
+      default:
+        return set_error(MBE_ERR_CUDA, "device status %d", ctl.status);
+    }
+  }
+  return MBE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,155 @@
+// Device-side types and warp helpers of the enumeration engine.
+#pragma once
+
+#include <cstdint>
+
+namespace gmbe {
+
+// Device status codes (negated MBE_ERR_* values are returned by the host).
+enum : int32_t {
+  kStOk = 0,
+  kStTimeout = 1,    // a bounded wait ran out
+  kStQueue = 2,      // queue slot never became valid
+  kStCapacity = 3,   // a scratch bound was exceeded
+};
+
+// Graph in HBM (internal numbering).  rev_* is the U -> V transpose.
+struct DevGraph {
+  int32_t nV, nU;
+  int64_t nE;
+  const int32_t* row_off;  // [nV+1]  V -> U
+  const int32_t* col;      // [nE]
+  const int32_t* rev_off;  // [nU+1]  U -> V
+  const int32_t* rev_col;  // [nE]
+  const uint64_t* ukey;    // [nU] hash key of internal U vertex (original id, original side)
+  const uint64_t* vkey;    // [nV]
+  int32_t swapped;         // internal U is the original V side
+  int32_t root_begin, root_end;  // roots [root_begin, root_end) are enumerated
+};
+
+// A task: up to four internal V vertices, -1 padded (reference LongTask,
+// src/GpuUtil.cuh:394-462).  Roots are one-vertex tasks.
+struct alignas(16) Task {
+  int32_t v[4];
+};
+
+// Global control block (one per launch).
+struct EnumCtl {
+  // results
+  unsigned long long count;
+  unsigned long long hash;
+  unsigned long long non_maximal;
+  unsigned long long tasks_split;
+  // scheduling
+  int32_t next_root;     // roots handed out so far (descending internal id)
+  int32_t status;        // first error code
+  int32_t abort;         // set together with status
+  int32_t pad0;
+  unsigned long long pending;   // queued + running tasks (termination)
+  unsigned long long q_head;    // next slot to consume
+  unsigned long long q_tail;    // next slot to produce
+  unsigned long long q_used;    // reserved and not yet consumed slots
+  unsigned long long err_info;  // diagnostic of the first error
+};
+
+// Per-warp scratch layout (int32 words unless noted), offsets in words from
+// the warp's base.  Built on the host from graph-derived capacities.
+struct ScratchLayout {
+  int64_t words_per_warp;
+  int32_t capC, capL, capS, kmax;
+  // offsets
+  int64_t map, touched, cv, ncnt, bound, coff, fill, sidx;
+  int64_t lv, llevel, lp, aoff, stack, lsize;
+  int64_t aadj, cadj;
+  int64_t masks, sub_v, bound2;
+  int64_t lkey, lmask, cursor2, sr2, nr2;  // lkey/sr2 are uint64 (8-byte aligned offsets)
+};
+
+struct EnumParams {
+  int32_t bound_height, bound_size, prune;
+  int32_t queue_cap;
+  int64_t slot_spin_limit;    // iterations waiting for a claimed slot to be written
+  int64_t idle_ns_limit;      // nanoseconds a warp may idle waiting for work
+  int32_t record_exit;        // -p
+  int32_t tier2_max_l;        // |L| at or below which the bitmap tier runs (<= 32*kmax)
+};
+
+__device__ __forceinline__ uint64_t fmix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+__device__ __forceinline__ uint64_t biclique_hash(const DevGraph& g, uint64_t sU, uint64_t nU,
+                                                  uint64_t sV, uint64_t nV) {
+  // Internal U is the L side; the canonical hash takes the original-U side first.
+  uint64_t sL = g.swapped ? sV : sU, nL = g.swapped ? nV : nU;
+  uint64_t sR = g.swapped ? sU : sV, nR = g.swapped ? nU : nV;
+  uint64_t rot = (sR << 29) | (sR >> 35);
+  return fmix64(sL ^ rot ^ ((nL << 32) | nR));
+}
+
+__device__ __forceinline__ unsigned lane_id() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%laneid;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ int warp_min_i(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ int warp_max_i(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Exclusive prefix sum within the warp.
+__device__ __forceinline__ int warp_excl_scan(int v, int* total) {
+  int lane = (int)lane_id();
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  *total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+// Lower bound: first index in a[0,n) with a[i] >= key.
+__device__ __forceinline__ int lower_bound_i(const int32_t* a, int n, int key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(a + mid) < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ bool contains_sorted(const int32_t* a, int n, int key) {
+  int p = lower_bound_i(a, n, key);
+  return p < n && __ldg(a + p) == key;
+}
+
+}  // namespace gmbe

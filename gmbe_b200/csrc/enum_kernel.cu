@@ -1,0 +1,1015 @@
+// The enumeration engine: one persistent kernel, one task per warp.
+//
+// Semantics follow the reference's GMBE path (the -s 2 kernel):
+//   task set-up      IterFinderWithMultipleVertex   src/IterFinderGpu.cu:772-887
+//   stack DFS        IterProcess                    src/IterFinderGpu.cu:12-69
+//   push / pop       finder_push / finder_pop       src/IterFinderGpu.h:206-303 (PRUNE_EN)
+//   task splitting   split test + LargeToTiny       src/IterFinderGpu.cu:835-858, 889-910
+//   scheduling       IterFinderKernel_6             src/IterFinderGpu.cu:918-1053
+// The data layout and the work per step are this engine's own:
+//   * Task set-up counts the two-hop multiset once through a per-warp dense
+//     map (no union merges, no binary searches) and lays the candidate set C
+//     out as [Q part | P part] instead of sorting it.
+//   * Tier 1 (|L| above the bitmap limit) keeps GMBE's per-candidate
+//     neighbour counts and level bounds, but walks per-task local adjacency
+//     (L position -> C index and C index -> L position) instead of binary
+//     searching global rows on every push and pop.
+//   * Tier 2 (|L| <= 32*K) re-expresses the same DFS over K-word bitmaps of
+//     the current L: a push is an AND, the maximality test a compare, the
+//     pro-active pruning test an AND with the removed vertices.
+//   * Split tasks go to a bounded MPMC ring; every device wait is bounded and
+//     reports a status instead of hanging.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "enum_common.cuh"
+#include "enum_launch.h"
+
+namespace gmbe {
+
+namespace {
+
+constexpr int32_t kFree = 0x7fffffff;     // live at every level (reference 0x7fff)
+constexpr int32_t kTouched = 0x3fffffff;  // marked by the pop restore pass (reference 0x3fff)
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(r));
+  return r;
+}
+
+__device__ void set_status(EnumCtl* ctl, int32_t code, unsigned long long info) {
+  if (atomicCAS(&ctl->status, 0, code) == 0) ctl->err_info = info;
+  atomicExch(&ctl->abort, 1);
+}
+
+// Visits every entry of a list of rows with all 32 lanes busy.  row_of(r, beg,
+// len) describes row r; visit(valid, r, pos) is called by every lane (uniform
+// control flow), pos indexing the global entry array.
+template <typename RowOf, typename Visit>
+__device__ __forceinline__ void flat_rows(int nr, RowOf row_of, Visit visit) {
+  const int lane = (int)lane_id();
+  for (int r0 = 0; r0 < nr; r0 += 32) {
+    int r = r0 + lane, beg = 0, len = 0;
+    if (r < nr) row_of(r, beg, len);
+    int tot;
+    int ex = warp_excl_scan(len, &tot);
+    for (int e0 = 0; e0 < tot; e0 += 32) {
+      int e = e0 + lane;
+      int lo = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        int cand = lo + step;
+        int exc = __shfl_sync(kFull, ex, cand & 31);
+        if (cand < 32 && exc <= e) lo = cand;
+      }
+      int b = __shfl_sync(kFull, beg, lo);
+      int exl = __shfl_sync(kFull, ex, lo);
+      bool valid = e < tot;
+      visit(valid, r0 + lo, b + (e - exl));
+    }
+  }
+}
+
+struct Warp {
+  DevGraph g;
+  EnumParams p;
+  ScratchLayout sl;
+  EnumCtl* ctl;
+  Task* q_tasks;
+  unsigned long long* q_seq;
+  int32_t* base;
+  // accumulators (uniform over lanes)
+  unsigned long long cnt, hash, nonmax, splits;
+
+  __device__ int32_t* A(int64_t off) const { return base + off; }
+  __device__ uint64_t* A64(int64_t off) const { return reinterpret_cast<uint64_t*>(base + off); }
+};
+
+// ---------------------------------------------------------------------------
+// Tier 2: bitmap DFS over a sub-problem with n <= 32*K vertices in L.
+//   masks[w*capC + i] : word w of candidate i's neighbourhood inside L
+//   subkey[i]         : hash key of candidate i
+//   candidates [0, nq) are Q (already excluded), [nq, nsub) are P.
+// Restates IterProcess / finder_push / finder_pop on bitmaps.
+template <int K>
+__device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
+  const int lane = (int)lane_id();
+  const int capC = W.sl.capC;
+  const uint32_t* masks = reinterpret_cast<const uint32_t*>(W.A(W.sl.masks));
+  const uint64_t* subkey = W.A64(W.sl.sub_v);
+  int32_t* bound = W.A(W.sl.bound2);
+  const uint64_t* lkey = W.A64(W.sl.lkey);
+  uint32_t* lmask = reinterpret_cast<uint32_t*>(W.A(W.sl.lmask));
+  int32_t* cursor = W.A(W.sl.cursor2);
+  const bool prune = W.p.prune != 0;
+
+  for (int i = lane; i < nsub; i += 32) bound[i] = kFree;
+  if (lane == 0) {
+    cursor[0] = nq;
+  }
+  if (lane < K) {
+    int bits = n - 32 * lane;
+    lmask[lane] = bits >= 32 ? 0xffffffffu : (bits <= 0 ? 0u : ((1u << bits) - 1u));
+  }
+  __syncwarp();
+  int level = 1;
+  while (level != 0) {
+    uint32_t Lm[K];
+#pragma unroll
+    for (int w = 0; w < K; ++w) Lm[w] = lmask[(level - 1) * K + w];
+    int cur = -1;
+    for (int b0 = cursor[level - 1]; b0 < nsub; b0 += 32) {
+      int i = b0 + lane;
+      bool ok = false;
+      if (i < nsub && bound[i] > level - 1) {
+        uint32_t any = 0;
+#pragma unroll
+        for (int w = 0; w < K; ++w) any |= masks[(size_t)w * capC + i] & Lm[w];
+        ok = any != 0;
+      }
+      unsigned bal = __ballot_sync(kFull, ok);
+      if (bal) {
+        cur = b0 + __ffs(bal) - 1;
+        break;
+      }
+    }
+    if (cur >= 0) {
+      // ---- push (finder_push) ----
+      uint32_t Ln[K];
+      int kn = 0;
+#pragma unroll
+      for (int w = 0; w < K; ++w) {
+        Ln[w] = Lm[w] & masks[(size_t)w * capC + cur];
+        kn += __popc(Ln[w]);
+      }
+      bool ism = true;
+      uint64_t sR = 0;
+      unsigned long long nR = 0;
+      for (int i = lane; i < nsub; i += 32) {
+        bool cover = true;
+#pragma unroll
+        for (int w = 0; w < K; ++w) cover &= (masks[(size_t)w * capC + i] & Ln[w]) == Ln[w];
+        if (cover) {
+          sR += subkey[i];
+          ++nR;
+          int b = bound[i];
+          if (i < cur && b >= level) ism = false;
+          else if (b > level) bound[i] = level;
+        }
+      }
+      ism = __all_sync(kFull, ism);
+      sR = warp_sum(sR) + sR0;
+      nR = warp_sum(nR) + nR0;
+      if (ism) {
+        uint64_t sL = 0;
+#pragma unroll
+        for (int w = 0; w < K; ++w)
+          if ((Ln[w] >> lane) & 1u) sL += lkey[w * 32 + lane];
+        sL = warp_sum(sL);
+        W.cnt += 1;
+        W.hash += biclique_hash(W.g, sL, (uint64_t)kn, sR, nR);
+      } else {
+        W.nonmax += 1;
+      }
+      __syncwarp();
+      if (ism && kn > 1) {
+        if (lane == 0) {
+          cursor[level - 1] = cur;
+          cursor[level] = cur + 1;
+        }
+        if (lane < K) {
+          uint32_t v = 0;
+#pragma unroll
+          for (int w = 0; w < K; ++w)
+            if (w == lane) v = Ln[w];
+          lmask[level * K + lane] = v;
+        }
+        __syncwarp();
+        ++level;
+        continue;
+      }
+      if (lane == 0) cursor[level - 1] = cur + 1;
+    } else {
+      --level;
+      if (level == 0) break;
+      cur = cursor[level - 1];
+      __syncwarp();
+      if (lane == 0) cursor[level - 1] = cur + 1;
+    }
+    // ---- pop (finder_pop) of candidate `cur` at `level` ----
+    uint32_t rem[K];
+    bool rem_any = false;
+#pragma unroll
+    for (int w = 0; w < K; ++w) {
+      uint32_t lp = lmask[(level - 1) * K + w];
+      rem[w] = lp & ~masks[(size_t)w * capC + cur];
+      rem_any |= rem[w] != 0;
+    }
+    (void)rem_any;
+    for (int i = lane; i < nsub; i += 32) {
+      int b = bound[i];
+      if (b >= level) {
+        if (prune) {
+          uint32_t t = 0;
+#pragma unroll
+          for (int w = 0; w < K; ++w) t |= masks[(size_t)w * capC + i] & rem[w];
+          bound[i] = (t != 0 || i == cur) ? kFree : level - 1;
+        } else {
+          bound[i] = kFree;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <int K>
+__device__ void tier2_dispatch_k(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
+  tier2_run<K>(W, n, nsub, nq, sR0, nR0);
+}
+
+__device__ void tier2(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
+  if (n <= 32) tier2_dispatch_k<1>(W, n, nsub, nq, sR0, nR0);
+  else if (n <= 64) tier2_dispatch_k<2>(W, n, nsub, nq, sR0, nR0);
+  else tier2_dispatch_k<4>(W, n, nsub, nq, sR0, nR0);
+}
+
+// Zeroes the masks of candidates [0, nsub) for n vertices.
+__device__ void clear_masks(Warp& W, int n, int nsub) {
+  const int lane = (int)lane_id();
+  int words = (n + 31) >> 5;
+  int kw = words <= 1 ? 1 : (words <= 2 ? 2 : 4);
+  uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+  for (int w = 0; w < kw; ++w)
+    for (int i = lane; i < nsub; i += 32) masks[(size_t)w * W.sl.capC + i] = 0u;
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Tier 1: GMBE counts + level bounds over the task's C, local adjacency.
+struct T1 {
+  const int32_t* L;   // L vertices (internal U ids)
+  int nL, nC, nq;
+  uint64_t sRtask, nRtask;
+};
+
+// Selects L positions with Llevel == lvl, calling fn(pos) over rows of aadj.
+template <typename Fn>
+__device__ __forceinline__ void t1_rows_at_level(Warp& W, const T1& t, int lvl, Fn fn) {
+  const int32_t* llevel = W.A(W.sl.llevel);
+  const int32_t* aoff = W.A(W.sl.aoff);
+  const int lane = (int)lane_id();
+  // Compact the selected rows of each 32-chunk, then walk them flat.
+  for (int c0 = 0; c0 < t.nL; c0 += 32) {
+    int l = c0 + lane;
+    bool sel = l < t.nL && llevel[l] == lvl;
+    unsigned bal = __ballot_sync(kFull, sel);
+    int nsel = __popc(bal);
+    if (nsel == 0) continue;
+    // Lane j takes the j-th selected row of the chunk (nsel <= 32, so the
+    // row index flat_rows passes to row_of is this lane's own id).
+    int myrow = -1;
+    {
+      unsigned m = bal;
+      for (int k = 0; k < lane && m; ++k) m &= m - 1;
+      if (lane < nsel) myrow = c0 + __ffs(m) - 1;
+    }
+    flat_rows(
+        nsel,
+        [&](int, int& beg, int& len) {
+          beg = aoff[myrow];
+          len = aoff[myrow + 1] - beg;
+        },
+        fn);
+  }
+}
+
+__device__ void t1_pop(Warp& W, const T1& t, int x, int level) {
+  int32_t* llevel = W.A(W.sl.llevel);
+  int32_t* ncnt = W.A(W.sl.ncnt);
+  int32_t* bound = W.A(W.sl.bound);
+  const int32_t* aadj = W.A(W.sl.aadj);
+  const int lane = (int)lane_id();
+  // restore counts over L_parent \ L_child and mark touched candidates
+  t1_rows_at_level(W, t, level - 1, [&](bool valid, int, int pos) {
+    if (!valid) return;
+    int p = aadj[pos];
+    if (p < 0) return;
+    atomicAdd(&ncnt[p], 1);
+    if (bound[p] >= level) bound[p] = kTouched;
+  });
+  __syncwarp();
+  for (int l = lane; l < t.nL; l += 32)
+    if (llevel[l] >= level) llevel[l] = level - 1;
+  __syncwarp();
+  if (W.p.prune) {
+    for (int i = lane; i < t.nC; i += 32) {
+      int b = bound[i];
+      if (b >= level) bound[i] = (b == kTouched || i == x) ? kFree : level - 1;
+    }
+  } else {
+    if (lane == 0) bound[x] = kFree;
+  }
+  __syncwarp();
+}
+
+// Hands the child sub-problem of a maximal push (x at `level`, |L_new| = kept)
+// to tier 2.  Candidates: C entries live below this level with
+// 0 < count < kept; Q = those before x.
+__device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uint64_t sR,
+                           uint64_t nR) {
+  const int lane = (int)lane_id();
+  const int32_t* llevel = W.A(W.sl.llevel);
+  const int32_t* ncnt = W.A(W.sl.ncnt);
+  const int32_t* bound = W.A(W.sl.bound);
+  const int32_t* cv = W.A(W.sl.cv);
+  int32_t* sidx = W.A(W.sl.sidx);
+  int32_t* lp = W.A(W.sl.lp);
+  uint64_t* lkey = W.A64(W.sl.lkey);
+  uint64_t* subkey = W.A64(W.sl.sub_v);
+  const int32_t* aoff = W.A(W.sl.aoff);
+  const int32_t* aadj = W.A(W.sl.aadj);
+  // L_sub positions
+  int n = 0;
+  for (int c0 = 0; c0 < t.nL; c0 += 32) {
+    int l = c0 + lane;
+    bool sel = l < t.nL && llevel[l] == level;
+    unsigned bal = __ballot_sync(kFull, sel);
+    if (sel) {
+      int j = n + __popc(bal & lanemask_lt());
+      lp[j] = l;
+      lkey[j] = W.g.ukey[t.L[l]];
+    }
+    n += __popc(bal);
+  }
+  // candidates
+  int nsub = 0, nq = 0;
+  for (int c0 = 0; c0 < t.nC; c0 += 32) {
+    int i = c0 + lane;
+    bool sel = false;
+    if (i < t.nC) {
+      int c = ncnt[i];
+      sel = bound[i] > level && c > 0 && c < kept;
+      sidx[i] = -1;
+    }
+    unsigned bal = __ballot_sync(kFull, sel);
+    if (sel) {
+      int s = nsub + __popc(bal & lanemask_lt());
+      sidx[i] = s;
+      subkey[s] = W.g.vkey[cv[i]];
+    }
+    nsub += __popc(bal);
+    // candidates before x are Q
+    unsigned before = __ballot_sync(kFull, sel && i < x);
+    nq += __popc(before);
+  }
+  __syncwarp();
+  if (nsub > 0) {
+    clear_masks(W, n, nsub);
+    uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+    const int capC = W.sl.capC;
+    flat_rows(
+        n,
+        [&](int r, int& beg, int& len) {
+          int l = lp[r];
+          beg = aoff[l];
+          len = aoff[l + 1] - beg;
+        },
+        [&](bool valid, int r, int pos) {
+          if (!valid) return;
+          int p = aadj[pos];
+          if (p < 0) return;
+          int s = sidx[p];
+          if (s >= 0) atomicOr(&masks[(size_t)(r >> 5) * capC + s], 1u << (r & 31));
+        });
+    __syncwarp();
+    tier2(W, n, nsub, nq, sR, nR);
+  }
+  __syncwarp();
+}
+
+__device__ void tier1_run(Warp& W, const T1& t) {
+  const int lane = (int)lane_id();
+  int32_t* llevel = W.A(W.sl.llevel);
+  int32_t* ncnt = W.A(W.sl.ncnt);
+  int32_t* bound = W.A(W.sl.bound);
+  int32_t* stack = W.A(W.sl.stack);
+  int32_t* lsize = W.A(W.sl.lsize);
+  const int32_t* cv = W.A(W.sl.cv);
+  const int32_t* coff = W.A(W.sl.coff);
+  const int32_t* cadj = W.A(W.sl.cadj);
+  const int32_t* aadj = W.A(W.sl.aadj);
+  const int t2max = W.p.tier2_max_l;
+
+  if (lane == 0) {
+    stack[0] = t.nq;
+    lsize[0] = t.nL;
+  }
+  __syncwarp();
+  int level = 1;
+  while (level != 0) {
+    int ab = lane == 0 ? *(volatile int32_t*)&W.ctl->abort : 0;
+    if (__shfl_sync(kFull, ab, 0)) return;
+    int cur = -1;
+    for (int b0 = stack[level - 1]; b0 < t.nC; b0 += 32) {
+      int i = b0 + lane;
+      bool ok = i < t.nC && bound[i] > level - 1 && ncnt[i] != 0;
+      unsigned bal = __ballot_sync(kFull, ok);
+      if (bal) {
+        cur = b0 + __ffs(bal) - 1;
+        break;
+      }
+    }
+    if (cur >= 0) {
+      // ---- finder_push (src/IterFinderGpu.h:206-264) ----
+      int kept = 0;
+      uint64_t sL = 0;
+      int rb = coff[cur], re = coff[cur + 1];
+      for (int j = rb + lane; j < re; j += 32) {
+        int l = cadj[j];
+        if (llevel[l] == level - 1) {
+          llevel[l] = level;
+          ++kept;
+          sL += W.g.ukey[t.L[l]];
+        }
+      }
+      kept = warp_sum(kept);
+      sL = warp_sum(sL);
+      __syncwarp();
+      int nLp = lsize[level - 1];
+      bool recompute = nLp > 2 * kept;
+      if (recompute) {
+        for (int i = lane; i < t.nC; i += 32) ncnt[i] = 0;
+        __syncwarp();
+        t1_rows_at_level(W, t, level, [&](bool valid, int, int pos) {
+          if (!valid) return;
+          int p = aadj[pos];
+          if (p >= 0) atomicAdd(&ncnt[p], 1);
+        });
+      } else {
+        t1_rows_at_level(W, t, level - 1, [&](bool valid, int, int pos) {
+          if (!valid) return;
+          int p = aadj[pos];
+          if (p >= 0) atomicSub(&ncnt[p], 1);
+        });
+      }
+      __syncwarp();
+      bool ism = true;
+      uint64_t sR = 0;
+      unsigned long long nR = 0;
+      for (int i = lane; i < t.nC; i += 32) {
+        if (ncnt[i] == kept) {
+          sR += W.g.vkey[cv[i]];
+          ++nR;
+          int b = bound[i];
+          if (i < cur && b >= level) ism = false;
+          else if (b > level) bound[i] = level;
+        }
+      }
+      ism = __all_sync(kFull, ism);
+      sR = warp_sum(sR) + t.sRtask;
+      nR = warp_sum(nR) + t.nRtask;
+      if (ism) {
+        W.cnt += 1;
+        W.hash += biclique_hash(W.g, sL, (uint64_t)kept, sR, nR);
+      } else {
+        W.nonmax += 1;
+      }
+      __syncwarp();
+      if (ism && kept > 1) {
+        if (kept <= t2max) {
+          t1_handoff(W, t, cur, level, kept, sR, nR);
+        } else {
+          if (lane == 0) {
+            stack[level - 1] = cur;
+            stack[level] = cur + 1;
+            lsize[level] = kept;
+          }
+          __syncwarp();
+          ++level;
+          continue;
+        }
+      }
+      if (lane == 0) stack[level - 1] = cur + 1;
+      __syncwarp();
+      t1_pop(W, t, cur, level);
+    } else {
+      --level;
+      if (level > 0) {
+        cur = stack[level - 1];
+        __syncwarp();
+        t1_pop(W, t, cur, level);
+        if (lane == 0) stack[level - 1] = cur + 1;
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Queue (bounded MPMC ring; replaces WorkList<LargeTask>, src/WorkList.cuh).
+//
+// Position gp lives in slot gp % cap during round gp / cap.  A slot's state
+// word is 2*round while it is free for that round's producer and 2*round+1
+// once the task is written; the consumer of position h hands the slot to the
+// next round by writing 2*(h/cap)+2.  q_used (reserved, not yet released
+// positions) never exceeds cap, so a producer only ever waits for a consumer
+// that has already claimed the older position and is reading it.
+__device__ __forceinline__ unsigned long long slot_free_tag(unsigned long long gp, int cap) {
+  return 2ULL * (gp / (unsigned long long)cap);
+}
+
+__device__ bool queue_pop(Warp& W, Task* out) {
+  // lane 0 only
+  EnumCtl* ctl = W.ctl;
+  volatile unsigned long long* vh = &ctl->q_head;
+  volatile unsigned long long* vt = &ctl->q_tail;
+  unsigned long long h = *vh;
+  if (h >= *vt) return false;
+  if (atomicCAS(&ctl->q_head, h, h + 1) != h) return false;
+  const int cap = W.p.queue_cap;
+  unsigned long long slot = h % (unsigned long long)cap;
+  volatile unsigned long long* st = W.q_seq + slot;
+  const unsigned long long full = slot_free_tag(h, cap) + 1;
+  int64_t spins = 0;
+  while (*st != full) {
+    if (++spins > W.p.slot_spin_limit) {
+      set_status(ctl, kStQueue, h);
+      return false;
+    }
+    __nanosleep(64);
+  }
+  __threadfence();
+  volatile int32_t* src = reinterpret_cast<volatile int32_t*>(W.q_tasks + slot);
+  out->v[0] = src[0];
+  out->v[1] = src[1];
+  out->v[2] = src[2];
+  out->v[3] = src[3];
+  __threadfence();
+  atomicExch(W.q_seq + slot, full + 1);  // free for round h/cap + 1
+  atomicAdd(&ctl->q_used, (unsigned long long)-1LL);
+  return true;
+}
+
+// Pushes children task + {cv[i]} for i in [nq, nC); false if the ring is full.
+__device__ bool queue_push_children(Warp& W, const Task& t, int k, int nq, int nC) {
+  const int lane = (int)lane_id();
+  EnumCtl* ctl = W.ctl;
+  const int cap = W.p.queue_cap;
+  unsigned long long n = (unsigned long long)(nC - nq);
+  unsigned long long pos = 0;
+  int ok = 0;
+  if (lane == 0) {
+    unsigned long long used = atomicAdd(&ctl->q_used, n);
+    if (used + n > (unsigned long long)cap) {
+      atomicAdd(&ctl->q_used, (unsigned long long)(-(long long)n));
+    } else {
+      atomicAdd(&ctl->pending, n);
+      pos = atomicAdd(&ctl->q_tail, n);
+      ok = 1;
+    }
+  }
+  ok = __shfl_sync(kFull, ok, 0);
+  if (!ok) return false;
+  pos = __shfl_sync(kFull, pos, 0);
+  const int32_t* cv = W.A(W.sl.cv);
+  for (int i = nq + lane; i < nC; i += 32) {
+    unsigned long long gp = pos + (unsigned long long)(i - nq);
+    unsigned long long slot = gp % (unsigned long long)cap;
+    volatile unsigned long long* st = W.q_seq + slot;
+    const unsigned long long free_tag = slot_free_tag(gp, cap);
+    int64_t spins = 0;
+    bool ready = true;
+    while (*st != free_tag) {
+      if (++spins > W.p.slot_spin_limit) {
+        set_status(ctl, kStQueue, gp);
+        ready = false;
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (!ready) continue;  // the run is aborting; the slot stays unwritten
+    Task c = t;
+    c.v[k] = cv[i];
+    W.q_tasks[slot] = c;
+    __threadfence();
+    atomicExch(W.q_seq + slot, free_tag + 1);
+  }
+  __syncwarp();
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Task set-up (IterFinderWithMultipleVertex) and dispatch.
+__device__ void run_task(Warp& W, const Task& t) {
+  const int lane = (int)lane_id();
+  const DevGraph& g = W.g;
+  int k = 1;
+  while (k < 4 && t.v[k] >= 0) ++k;
+  const int last = t.v[k - 1];
+  int32_t* map = W.A(W.sl.map);
+  int32_t* touched = W.A(W.sl.touched);
+  int32_t* lv = W.A(W.sl.lv);
+
+  // ---- L = common neighbours of the task vertices ----
+  const int32_t* L;
+  int nL;
+  if (k == 1) {
+    L = g.col + g.row_off[last];
+    nL = g.row_off[last + 1] - g.row_off[last];
+  } else {
+    // Intersect: probe the smallest row against the others.
+    int best = 0, bestlen = 0x7fffffff;
+    for (int i = 0; i < k; ++i) {
+      int len = g.row_off[t.v[i] + 1] - g.row_off[t.v[i]];
+      if (len < bestlen) {
+        bestlen = len;
+        best = i;
+      }
+    }
+    const int32_t* sm = g.col + g.row_off[t.v[best]];
+    int n = 0;
+    for (int b0 = 0; b0 < bestlen; b0 += 32) {
+      int j = b0 + lane;
+      bool in = j < bestlen;
+      int u = in ? __ldg(sm + j) : 0;
+      for (int i = 0; i < k && in; ++i) {
+        if (i == best) continue;
+        const int32_t* row = g.col + g.row_off[t.v[i]];
+        in = contains_sorted(row, g.row_off[t.v[i] + 1] - g.row_off[t.v[i]], u);
+      }
+      unsigned bal = __ballot_sync(kFull, in);
+      if (in) lv[n + __popc(bal & lanemask_lt())] = u;
+      n += __popc(bal);
+    }
+    __syncwarp();
+    L = lv;
+    nL = n;
+  }
+  if (nL == 0) return;
+  if (nL > W.sl.capL) {
+    set_status(W.ctl, kStCapacity, ((unsigned long long)1 << 32) | (unsigned)nL);
+    return;
+  }
+
+  // ---- two-hop multiset: counts in the per-warp dense map ----
+  int32_t* aoff = W.A(W.sl.aoff);
+  {
+    int run = 0;
+    for (int c0 = 0; c0 < nL; c0 += 32) {
+      int l = c0 + lane;
+      int d = 0;
+      if (l < nL) {
+        int u = L[l];
+        d = g.rev_off[u + 1] - g.rev_off[u];
+      }
+      int tot;
+      int ex = warp_excl_scan(d, &tot);
+      if (l < nL) aoff[l] = run + ex;
+      run += tot;
+    }
+    if (lane == 0) aoff[nL] = run;
+    if (run > W.sl.capS) {
+      set_status(W.ctl, kStCapacity, ((unsigned long long)2 << 32) | (unsigned)run);
+      return;
+    }
+  }
+  __syncwarp();
+  int nt = 0;
+  flat_rows(
+      nL,
+      [&](int r, int& beg, int& len) {
+        int u = L[r];
+        beg = g.rev_off[u];
+        len = g.rev_off[u + 1] - beg;
+      },
+      [&](bool valid, int, int pos) {
+        int w = valid ? __ldg(g.rev_col + pos) : 0;
+        int old = valid ? atomicAdd(&map[w], 1) : 1;
+        bool isnew = valid && old == 0;
+        unsigned bal = __ballot_sync(kFull, isnew);
+        if (isnew) touched[nt + __popc(bal & lanemask_lt())] = w;
+        nt += __popc(bal);
+      });
+  __syncwarp();
+  if (nt > W.sl.capC) {
+    set_status(W.ctl, kStCapacity, ((unsigned long long)3 << 32) | (unsigned)nt);
+    for (int i = lane; i < nt && i < W.sl.capC; i += 32) map[touched[i]] = 0;
+    return;
+  }
+
+  // ---- classify: R (count == |L|), Q (w < last), P (w > last) ----
+  int32_t* cv = W.A(W.sl.cv);
+  int32_t* ncnt = W.A(W.sl.ncnt);
+  int32_t* bound = W.A(W.sl.bound);
+  uint64_t sR = 0;
+  unsigned long long nR = 0;
+  int nq = 0, np = 0;
+  int viol_first = 0x7fffffff;  // smallest R vertex below `last` (maximality witnesses)
+  int nC = 0;
+  {
+    // count C size first so P can fill from the back
+    int cntC = 0;
+    for (int b0 = 0; b0 < nt; b0 += 32) {
+      int i = b0 + lane;
+      bool isC = i < nt && map[touched[i]] != nL;
+      cntC += __popc(__ballot_sync(kFull, isC));
+    }
+    nC = cntC;
+  }
+  for (int b0 = 0; b0 < nt; b0 += 32) {
+    int i = b0 + lane;
+    bool valid = i < nt;
+    int w = valid ? touched[i] : 0;
+    int c = valid ? map[w] : 0;
+    bool isR = valid && c == nL;
+    bool isQ = valid && !isR && w < last;
+    bool isP = valid && !isR && w > last;
+    if (isR) {
+      sR += g.vkey[w];
+      ++nR;
+      if (w < last) viol_first = min(viol_first, w);
+    }
+    unsigned bq = __ballot_sync(kFull, isQ);
+    unsigned bp = __ballot_sync(kFull, isP);
+    int pos = -1;
+    if (isQ) pos = nq + __popc(bq & lanemask_lt());
+    if (isP) pos = nC - 1 - (np + __popc(bp & lanemask_lt()));
+    if (pos >= 0) {
+      cv[pos] = w;
+      ncnt[pos] = c;
+      bound[pos] = kFree;
+      map[w] = pos + 1;
+    } else if (valid) {
+      map[w] = 0;
+    }
+    nq += __popc(bq);
+    np += __popc(bp);
+  }
+  sR = warp_sum(sR);
+  nR = warp_sum(nR);
+  viol_first = warp_min_i(viol_first);
+  __syncwarp();
+
+  // ---- maximality of the task (src/IterFinderGpu.cu:800-822) ----
+  bool ism = true;
+  if (viol_first != 0x7fffffff) {
+    if (k == 1) {
+      ism = false;  // R[0] != root
+    } else {
+      // Every R vertex below `last` must already cover L_parent.
+      int32_t* lp = W.A(W.sl.lp);
+      const int32_t* Lpar;
+      int nLp;
+      if (k == 2) {
+        Lpar = g.col + g.row_off[t.v[0]];
+        nLp = g.row_off[t.v[0] + 1] - g.row_off[t.v[0]];
+      } else {
+        const int32_t* r0 = g.col + g.row_off[t.v[0]];
+        int len0 = g.row_off[t.v[0] + 1] - g.row_off[t.v[0]];
+        int n = 0;
+        for (int b0 = 0; b0 < len0; b0 += 32) {
+          int j = b0 + lane;
+          bool in = j < len0;
+          int u = in ? __ldg(r0 + j) : 0;
+          for (int i = 1; i < k - 1 && in; ++i)
+            in = contains_sorted(g.col + g.row_off[t.v[i]],
+                                 g.row_off[t.v[i] + 1] - g.row_off[t.v[i]], u);
+          unsigned bal = __ballot_sync(kFull, in);
+          if (in) lp[n + __popc(bal & lanemask_lt())] = u;
+          n += __popc(bal);
+        }
+        __syncwarp();
+        Lpar = lp;
+        nLp = n;
+      }
+      for (int b0 = 0; b0 < nt && ism; b0 += 32) {
+        int i = b0 + lane;
+        int w = i < nt ? touched[i] : 0;
+        bool cand = i < nt && w < last && map[w] == 0;  // R vertex below last
+        // (map[w] == 0 marks R after classification)
+        unsigned bal = __ballot_sync(kFull, cand);
+        while (bal && ism) {
+          int src = __ffs(bal) - 1;
+          bal &= bal - 1;
+          int ww = __shfl_sync(kFull, w, src);
+          bool trivially = false;
+          for (int q = 0; q < k - 1; ++q) trivially |= (t.v[q] == ww);
+          if (trivially) continue;
+          const int32_t* rw = g.col + g.row_off[ww];
+          int dw = g.row_off[ww + 1] - g.row_off[ww];
+          bool all = true;
+          for (int j = lane; j < nLp; j += 32) all &= contains_sorted(rw, dw, Lpar[j]);
+          if (!__all_sync(kFull, all)) ism = false;
+        }
+      }
+    }
+  }
+  if (!ism) {
+    W.nonmax += 1;
+    for (int i = lane; i < nt; i += 32) map[touched[i]] = 0;
+    __syncwarp();
+    return;
+  }
+  // the task's own biclique
+  {
+    uint64_t sL = 0;
+    for (int l = lane; l < nL; l += 32) sL += g.ukey[L[l]];
+    sL = warp_sum(sL);
+    W.cnt += 1;
+    W.hash += biclique_hash(g, sL, (uint64_t)nL, sR, nR);
+  }
+  bool done = nL <= 1 || np == 0;
+  // ---- split (src/IterFinderGpu.cu:835-858) ----
+  if (!done && k < 4) {
+    long long rest = np;
+    if ((rest > W.p.bound_height || nL > W.p.bound_height) &&
+        rest * (long long)nL > (long long)W.p.bound_size) {
+      if (queue_push_children(W, t, k, nq, nC)) {
+        W.splits += 1;
+        done = true;
+      }
+    }
+  }
+  if (!done) {
+    if (nL <= W.p.tier2_max_l) {
+      // ---- tier 2 directly: masks of every candidate over all of L ----
+      uint64_t* lkey = W.A64(W.sl.lkey);
+      uint64_t* subkey = W.A64(W.sl.sub_v);
+      for (int l = lane; l < nL; l += 32) lkey[l] = g.ukey[L[l]];
+      for (int i = lane; i < nC; i += 32) subkey[i] = g.vkey[cv[i]];
+      clear_masks(W, nL, nC);
+      uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+      const int capC = W.sl.capC;
+      flat_rows(
+          nL,
+          [&](int r, int& beg, int& len) {
+            int u = L[r];
+            beg = g.rev_off[u];
+            len = g.rev_off[u + 1] - beg;
+          },
+          [&](bool valid, int r, int pos) {
+            if (!valid) return;
+            int p = map[__ldg(g.rev_col + pos)] - 1;
+            if (p >= 0) atomicOr(&masks[(size_t)(r >> 5) * capC + p], 1u << (r & 31));
+          });
+      __syncwarp();
+      tier2(W, nL, nC, nq, sR, nR);
+    } else {
+      // ---- tier 1: local adjacency ----
+      int32_t* llevel = W.A(W.sl.llevel);
+      int32_t* aadj = W.A(W.sl.aadj);
+      int32_t* coff = W.A(W.sl.coff);
+      int32_t* fill = W.A(W.sl.fill);
+      int32_t* cadj = W.A(W.sl.cadj);
+      int32_t* sidx = W.A(W.sl.sidx);
+      for (int l = lane; l < nL; l += 32) llevel[l] = 0;
+      // aadj: L row -> C index (or -1 for R), rows sized by degree
+      flat_rows(
+          nL,
+          [&](int r, int& beg, int& len) {
+            int u = L[r];
+            beg = g.rev_off[u];
+            len = g.rev_off[u + 1] - beg;
+          },
+          [&](bool valid, int r, int pos) {
+            if (!valid) return;
+            int u = L[r];
+            int off = aoff[r] + (pos - g.rev_off[u]);
+            aadj[off] = map[__ldg(g.rev_col + pos)] - 1;
+          });
+      // coff = exclusive scan of the initial counts; fill = 0; sidx = -1
+      {
+        int run = 0;
+        for (int c0 = 0; c0 < nC; c0 += 32) {
+          int i = c0 + lane;
+          int c = i < nC ? ncnt[i] : 0;
+          int tot;
+          int ex = warp_excl_scan(c, &tot);
+          if (i < nC) {
+            coff[i] = run + ex;
+            fill[i] = 0;
+            sidx[i] = -1;
+          }
+          run += tot;
+        }
+        if (lane == 0) coff[nC] = run;
+      }
+      __syncwarp();
+      // cadj: C index -> L positions
+      flat_rows(
+          nL,
+          [&](int r, int& beg, int& len) {
+            beg = aoff[r];
+            len = aoff[r + 1] - beg;
+          },
+          [&](bool valid, int r, int pos) {
+            if (!valid) return;
+            int p = aadj[pos];
+            if (p < 0) return;
+            int s = atomicAdd(&fill[p], 1);
+            cadj[coff[p] + s] = r;
+          });
+      __syncwarp();
+      T1 t1;
+      t1.L = L;
+      t1.nL = nL;
+      t1.nC = nC;
+      t1.nq = nq;
+      t1.sRtask = sR;
+      t1.nRtask = nR;
+      tier1_run(W, t1);
+    }
+  }
+  __syncwarp();
+  for (int i = lane; i < nt; i += 32) map[touched[i]] = 0;
+  __syncwarp();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kEnumThreads, 1)
+    mbe_enum_kernel(DevGraph g, EnumParams p, ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
+                    unsigned long long* q_seq, int32_t* scratch, unsigned long long* exit_ns) {
+  uint64_t t_start = globaltimer_ns();
+  const int lane = (int)lane_id();
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  Warp W;
+  W.g = g;
+  W.p = p;
+  W.sl = sl;
+  W.ctl = ctl;
+  W.q_tasks = q_tasks;
+  W.q_seq = q_seq;
+  W.base = scratch + (size_t)warp_global * (size_t)sl.words_per_warp;
+  W.cnt = W.hash = W.nonmax = W.splits = 0;
+  const int nroots = g.root_end - g.root_begin;
+  uint64_t idle_since = 0;
+  while (true) {
+    int ab = lane == 0 ? *(volatile int32_t*)&ctl->abort : 0;
+    if (__shfl_sync(kFull, ab, 0)) break;
+    Task t;
+    int have = 0;
+    if (lane == 0) {
+      have = queue_pop(W, &t) ? 1 : 0;
+      if (!have && *(volatile int32_t*)&ctl->next_root < nroots) {
+        atomicAdd(&ctl->pending, 1ULL);
+        int r = atomicAdd(&ctl->next_root, 1);
+        if (r < nroots) {
+          t.v[0] = g.root_end - 1 - r;
+          t.v[1] = t.v[2] = t.v[3] = -1;
+          have = 1;
+        } else {
+          atomicAdd(&ctl->pending, (unsigned long long)-1LL);
+        }
+      }
+    }
+    have = __shfl_sync(kFull, have, 0);
+    if (have) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) t.v[i] = __shfl_sync(kFull, t.v[i], 0);
+      run_task(W, t);
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence();
+        atomicAdd(&ctl->pending, (unsigned long long)-1LL);
+      }
+      idle_since = 0;
+      continue;
+    }
+    int finished = 0;
+    if (lane == 0) {
+      finished = (*(volatile int32_t*)&ctl->next_root >= nroots &&
+                  *(volatile unsigned long long*)&ctl->pending == 0ULL)
+                     ? 1
+                     : 0;
+    }
+    finished = __shfl_sync(kFull, finished, 0);
+    if (finished) break;
+    uint64_t now = globaltimer_ns();
+    if (idle_since == 0) {
+      idle_since = now;
+    } else if (now - idle_since > (uint64_t)p.idle_ns_limit) {
+      if (lane == 0) set_status(ctl, kStTimeout, now - idle_since);
+      break;
+    }
+    __nanosleep(256);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    if (W.cnt) atomicAdd(&ctl->count, W.cnt);
+    if (W.hash) atomicAdd(&ctl->hash, W.hash);
+    if (W.nonmax) atomicAdd(&ctl->non_maximal, W.nonmax);
+    if (W.splits) atomicAdd(&ctl->tasks_split, W.splits);
+  }
+  if (p.record_exit) {
+    __syncthreads();
+    if (threadIdx.x == 0) exit_ns[blockIdx.x] = globaltimer_ns() - t_start;
+  }
+}
+
+}  // namespace gmbe

@@ -1,0 +1,186 @@
+/*
+ * mbe.h -- C ABI of the B200 maximal biclique enumeration (MBE) engine.
+ *
+ * This is the drop-in boundary for the single-GPU GMBE hot path
+ * (`MBE_GPU -s 2`).  The reference exposes that path only as C++ classes:
+ *   - CSRBiGraph::Read / CopyToGpu / Reset      (src/BiGraph.h:23-38, src/BiGraph.cu:13-278, 413-454)
+ *   - IterFinderGpu6(graph, bound_height, bound_size), Execute()   (src/IterFinderGpu.h:77-90,
+ *     src/IterFinderGpu.cu:1056-1119)
+ *   - BicliqueFinder::PrintResult                 (src/BicliqueFinder.cu:9-16)
+ * Every entry point below names the reference interface it replaces.  The C++
+ * classes with the reference's names (CSRBiGraph, IterFinderGpu6, ...) are
+ * provided on top of this ABI by include/mbe_finder.h.
+ *
+ * Conventions
+ *   - Every function returns an int status: MBE_OK (0) or a negative MBE_ERR_*.
+ *     The reference exits the process on any CUDA error (gpuErrchk,
+ *     src/Utility.h:30-39); this ABI reports instead, and mbe_last_error_string()
+ *     gives the message of the calling thread's last failure.
+ *   - Plain pointers and sizes only.  Vertex ids are int32, edge counts int64,
+ *     counters uint64 (the reference's `int maximal_nodes_` wraps past 2^31).
+ *   - A graph handle owns host and device copies of the CSR.  One handle may be
+ *     used by one host thread at a time.
+ *
+ * Biclique identity and the set hash
+ *   A maximal biclique is (L, R), L a set of U ids (the integers on an .adj
+ *   line), R a set of V ids (0-based .adj line numbers), L = N(R), R = N(L),
+ *   both non-empty.  Ids are always the ORIGINAL input ids, whatever side swap
+ *   (-t) or row ordering (-o) was applied internally.  The set hash is
+ *     key_U(u) = fmix64(2u), key_V(v) = fmix64(2v+1)      (MurmurHash3 fmix64)
+ *     sL = sum key_U(u), sR = sum key_V(v)                 (mod 2^64)
+ *     H(L,R) = fmix64(sL ^ rotl64(sR,29) ^ (|L|<<32 | |R|))
+ *     set_hash = sum over all maximal bicliques of H      (mod 2^64)
+ */
+#ifndef GMBE_B200_MBE_H
+#define GMBE_B200_MBE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MBE_OK 0
+#define MBE_ERR_INVALID (-1)    /* bad argument */
+#define MBE_ERR_IO (-2)         /* file cannot be opened or read */
+#define MBE_ERR_FORMAT (-3)     /* .adj row not ascending/unique, empty row, bad token, id >= 2^31 */
+#define MBE_ERR_CUDA (-4)       /* CUDA runtime error */
+#define MBE_ERR_NOMEM (-5)      /* host or device allocation failed */
+#define MBE_ERR_TIMEOUT (-6)    /* a bounded device wait ran out */
+#define MBE_ERR_QUEUE_FULL (-7) /* device worklist capacity exceeded */
+#define MBE_ERR_CAPACITY (-8)   /* a per-warp scratch bound was exceeded */
+#define MBE_ERR_ADMISSION (-9)  /* serving: request can never fit the arena */
+#define MBE_ERR_CANCELLED (-10) /* serving: request cancelled */
+#define MBE_ERR_NOT_FOUND (-11) /* serving: unknown request id */
+#define MBE_ERR_AGAIN (-12)     /* serving: result not ready yet */
+
+/* ---- options (reference: struct Option, src/BiGraph.h:13-22) ------------ */
+typedef struct mbe_opts {
+  int32_t uvtrans;   /* -t: 0 keep sides; 1 make V the smaller side; 2 the larger */
+  int32_t order;     /* -o: 0 input order; 1 V rows by (size asc, lexicographic); 2 size desc */
+  int32_t fast_mode; /* -f: 1 skips the two-hop degree statistics */
+  int32_t device;    /* CUDA device ordinal (the reference always uses device 0) */
+} mbe_opts;
+
+/* ---- graph summary (reference: CSRBiGraph fields, src/BiGraph.h:30) ---- */
+typedef struct mbe_graph_info {
+  int32_t U_size, V_size;  /* internal sides, after the -t swap */
+  int64_t edge_size;
+  int32_t U_degree, V_degree;   /* max degrees */
+  int32_t U_2degree, V_2degree; /* max two-hop degrees (0 under fast_mode) */
+  int32_t swapped;              /* 1 if -t swapped U and V */
+} mbe_graph_info;
+
+/* ---- enumeration parameters (reference: IterFinderGpu6 ctor args and the
+ *      compile-time switches PRUNE_EN / WARP_PER_BLOCK, src/CMakeLists.txt) */
+typedef struct mbe_params {
+  int32_t bound_height;    /* -m (default 20): a task is split when (|P| > h or |L| > h) ... */
+  int32_t bound_size;      /* -n (default 1500): ... and |P|*|L| > bound_size (|P| = C - next) */
+  int32_t prune;           /* 1 = pro-active pruning (PRUNE_EN, default), 0 = off */
+  int32_t blocks;          /* persistent grid size, 0 = SM count x occupancy */
+  int32_t queue_capacity;  /* split-task ring entries, 0 = sized from the graph */
+  int32_t bitmap_max_l;    /* bitmap tier for |L| <= this (<= 128); 0 = 128; -1 = counts tier only */
+  int64_t wait_limit_ns;   /* longest a warp may idle waiting for work, 0 = 600 s */
+  int32_t sm_timing;       /* -p: record each block's exit time */
+  int32_t root_begin;      /* enumerate only roots [root_begin, root_end) of the internal */
+  int32_t root_end;        /*   order (0, 0 = all); the internal order is -t/-o applied   */
+  int32_t reserved;
+} mbe_params;
+
+typedef struct mbe_result {
+  uint64_t count;        /* number of maximal bicliques */
+  uint64_t set_hash;     /* order-independent canonical set hash (see above) */
+  uint64_t non_maximal;  /* branches rejected by the maximality check */
+  uint64_t tasks_split;  /* tasks expanded through the split queue */
+  double enum_seconds;   /* host wall time of mbe_enumerate (reference: exe_time_) */
+  float kernel_ms;       /* CUDA-event time of the enumeration kernel(s) */
+  int32_t status;        /* device status word (0 = OK) */
+  double sm_exit_max_ms; /* -p: slowest block's exit time, ms after launch */
+  double sm_exit_min_ms; /* -p: fastest block's exit time */
+} mbe_result;
+
+/* Default parameters: bound_height 20, bound_size 1500, prune 1. */
+void mbe_params_default(mbe_params* p);
+void mbe_opts_default(mbe_opts* o);
+
+/* ---- graph lifetime ----------------------------------------------------- */
+typedef struct mbe_graph mbe_graph;
+
+/* Parse an .adj file and upload it.  Replaces CSRBiGraph::Read
+ * (src/BiGraph.cu:13-278) followed by CopyToGpu (src/BiGraph.cu:413-431).
+ * Unlike the reference, a row that is not strictly ascending, an empty row
+ * or an id >= 2^31-1 is reported as MBE_ERR_FORMAT, and a missing file as
+ * MBE_ERR_IO (the reference prints "Can't open file" and continues with an
+ * empty graph). */
+int mbe_graph_from_adj(const char* path, const mbe_opts* opts, mbe_graph** out);
+
+/* Build a graph from an .adj-shaped CSR in host memory: row v (0..nV-1) holds
+ * the U ids col[row_off[v] .. row_off[v+1]).  nU = 0 means max id + 1, as the
+ * reference computes U_size (src/BiGraph.cu:31).  Same checks as above.
+ * Replaces the in-memory half of CSRBiGraph::Read plus CopyToGpu. */
+int mbe_graph_from_csr(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t nU,
+                       int64_t nE, const mbe_opts* opts, mbe_graph** out);
+
+int mbe_graph_get_info(const mbe_graph* g, mbe_graph_info* info);
+
+/* Release host and device memory.  Replaces CSRBiGraph::Reset (src/BiGraph.cu:433-454). */
+int mbe_graph_free(mbe_graph* g);
+
+/* ---- enumeration --------------------------------------------------------- */
+/* Count all maximal bicliques of g and their set hash on g's device.
+ * Replaces IterFinderGpu6::IterFinderGpu6 + Execute (src/IterFinderGpu.cu:1056-1119).
+ * `params` may be NULL (defaults).  Synchronous on the calling thread. */
+int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out);
+
+/* Thread-local message of the last failed call ("" if none). */
+const char* mbe_last_error_string(void);
+
+/* ---- synthetic inputs ------------------------------------------------------
+ * Seeded Chung-Lu bipartite generator (splitmix64 stream, Vose alias
+ * sampling): expected degree of vertex i proportional to (i+1)^(-1/(gamma-1)),
+ * capped at max_deg, scaled to ~n_edges; duplicate edges removed, rows sorted,
+ * V rows of degree 0 dropped and U ids renumbered densely (so every vertex of
+ * either side has an edge).  pair_p_max > 0 caps the probability of any one
+ * (u,v) pair at pair_p_max: a draw is kept with probability
+ * min(1, -ln(1-pair_p_max) / (w_u w_v / sum w)).  Without the cap, hubs whose
+ * weight product exceeds the edge count form a near-complete block whose few
+ * missing edges give exponentially many maximal bicliques.
+ * Optional planted blocks: n_blocks disjoint (block_u x block_v) vertex sets,
+ * each pair an edge with probability block_p.  Not part of the reference
+ * (its inputs are downloaded datasets, preprocess/prepare_dataset.sh). */
+typedef struct mbe_gen_spec {
+  int64_t nU, nV, n_edges;
+  double gamma_u, gamma_v;
+  int64_t max_deg_u, max_deg_v;
+  uint64_t seed;
+  int32_t n_blocks, block_u, block_v, reserved;
+  double block_p;
+  double pair_p_max; /* 0 = uncapped Chung-Lu */
+} mbe_gen_spec;
+
+/* Generate into library-owned arrays (release with mbe_free). *row_off has
+ * *nV+1 entries, *col has *nE entries. */
+int mbe_gen_chung_lu(const mbe_gen_spec* spec, int32_t** row_off, int32_t** col, int32_t* nV,
+                     int32_t* nU, int64_t* nE);
+
+/* The batched-mode size distribution: from `seed`, |U| log-uniform in
+ * [50, 5000], |V|/|U| log-uniform in [0.5, 4], average U degree uniform in
+ * [3, 30], exponent 2.2 on both sides, pair probability cap 0.1. */
+int mbe_gen_batch_spec(uint64_t seed, mbe_gen_spec* out);
+
+/* Write an .adj file (one line per V row, space-separated ascending U ids). */
+int mbe_write_adj(const char* path, const int32_t* row_off, const int32_t* col, int32_t nV);
+
+/* Parse an .adj file into library-owned host arrays without uploading. */
+int mbe_read_adj(const char* path, int32_t** row_off, int32_t** col, int32_t* nV, int32_t* nU,
+                 int64_t* nE);
+
+void mbe_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GMBE_B200_MBE_H */

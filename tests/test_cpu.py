@@ -1,0 +1,218 @@
+"""CPU-only tests: the oracle against the reference's golden results, host
+logic (generator, .adj I/O, input validation) and the C-ABI library's
+exports.  No compute call here needs a GPU."""
+import ctypes
+import hashlib
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from util import planted, random_bipartite
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden", "golden.json")
+
+
+@pytest.fixture(scope="module")
+def gm():
+    import gmbe_b200
+    return gmbe_b200
+
+
+def _digest(ro, co):
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(ro, np.int32).tobytes())
+    h.update(np.ascontiguousarray(co, np.int32).tobytes())
+    return h.hexdigest()[:16]
+
+
+# ---------------------------------------------------------------------------
+# The C ABI library exports every function the headers declare.
+
+def _declared_functions():
+    names = []
+    hdr = open(os.path.join(ROOT, "include", "mbe.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b(mbe_\w+)\s*\(", hdr, flags=re.M):
+        names.append(m.group(1))
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(gm):
+    names = _declared_functions()
+    assert len(names) >= 12
+    lib = ctypes.CDLL(gm.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_cpp_classes_exported(gm):
+    out = subprocess.run(["nm", "-DC", gm.LIB_PATH], capture_output=True, text=True).stdout
+    for sym in ("CSRBiGraph::Read", "IterFinderGpu6::Execute", "BicliqueFinder::PrintResult",
+                "IterFinderGpu6::IterFinderGpu6"):
+        assert sym in out, sym
+
+
+def test_cli_built(gm):
+    assert os.access(gm.CLI_PATH, os.X_OK)
+
+
+# ---------------------------------------------------------------------------
+# Oracle pinned against the reference's own enumerators (golden fixtures).
+
+def _golden_cases():
+    with open(GOLDEN) as f:
+        return {c["name"]: c for c in json.load(f)["cases"]}
+
+
+def _case_graph(gm, name):
+    if name.startswith("tiny_random_"):
+        return random_bipartite(40, 48, 0.25, int(name.rsplit("_", 1)[1]))
+    if name == "planted_300x200":
+        return planted(300, 200, blocks=6, seed=3, bsize=14)
+    if name == "config_small":
+        g = gm.config_graph("small")
+        return g.row_off, g.col, g.nU
+    if name.startswith("batch_"):
+        g = gm.batch_graph(int(name.split("_")[1]))
+        return g.row_off, g.col, g.nU
+    if name == "config_medium":
+        g = gm.config_graph("medium")
+        return g.row_off, g.col, g.nU
+    raise KeyError(name)
+
+
+@pytest.mark.parametrize("name", [n for n in _golden_cases() if n != "config_medium"])
+def test_oracle_matches_reference_golden(gm, name):
+    c = _golden_cases()[name]
+    ro, co, nU = _case_graph(gm, name)
+    assert _digest(ro, co) == c["csr_sha256_16"], "generator output changed"
+    o = oracle.gmbe(ro, co, nU)
+    for label, ref in c["reference"].items():
+        if ref.get("count") is not None:
+            assert o.count == ref["count"], label
+    assert f"{o.set_hash:#018x}" == c["oracle_set_hash"]
+    if "brute_force_set_hash" in c:
+        bf = oracle.brute_force(ro, co, nU)
+        assert f"{bf.set_hash:#018x}" == c["brute_force_set_hash"] == c["oracle_set_hash"]
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_three_oracles_agree(seed):
+    ro, co, nU = random_bipartite(30 + seed, 24 + 4 * seed, 0.3, seed)
+    bf = oracle.brute_force(ro, co, nU)
+    mb = oracle.mbea(ro, co, nU)
+    for uvtrans, order, prune in ((0, 0, 1), (1, 1, 1), (2, 2, 0), (0, 1, 0)):
+        gmr = oracle.gmbe(ro, co, nU, uvtrans=uvtrans, order=order, prune=prune, threads=2)
+        assert (gmr.count, gmr.set_hash) == (bf.count, bf.set_hash)
+    assert (mb.count, mb.set_hash) == (bf.count, bf.set_hash)
+
+
+def test_oracle_root_ranges_are_additive():
+    ro, co, nU = planted(200, 150, blocks=4, seed=2)
+    full = oracle.gmbe(ro, co, nU)
+    nV_int = min(len(ro) - 1, nU)  # uvtrans=1: the smaller side holds the roots
+    a = oracle.gmbe_range(ro, co, nU, 0, nV_int // 2)
+    b = oracle.gmbe_range(ro, co, nU, nV_int // 2, nV_int)
+    assert a.count + b.count == full.count
+    assert (a.set_hash + b.set_hash) % (1 << 64) == full.set_hash
+
+
+def test_hash_detects_a_planted_mistake():
+    # Dropping one edge changes the set of maximal bicliques, and the hash
+    # must see it even when the count happens to stay the same.
+    ro, co, nU = random_bipartite(20, 20, 0.4, 1)
+    base = oracle.brute_force(ro, co, nU)
+    co2 = co.copy()
+    row = 3
+    keep = np.ones(len(co2), bool)
+    keep[ro[row]] = False
+    if ro[row + 1] - ro[row] == 1:
+        pytest.skip("row has one edge")
+    ro2 = ro.copy()
+    ro2[row + 1:] -= 1
+    mut = oracle.brute_force(ro2, co2[keep], nU)
+    assert mut.set_hash != base.set_hash
+
+
+# ---------------------------------------------------------------------------
+# Host logic: generator, .adj I/O, validation.
+
+def test_generator_is_deterministic_and_clean(gm):
+    a = gm.config_graph("small")
+    b = gm.config_graph("small")
+    assert np.array_equal(a.row_off, b.row_off) and np.array_equal(a.col, b.col)
+    deg = np.diff(a.row_off)
+    assert deg.min() >= 1  # no empty .adj line
+    assert deg.max() <= 400
+    for v in range(a.nV):
+        r = a.col[a.row_off[v]:a.row_off[v + 1]]
+        assert np.all(np.diff(r) > 0)
+    assert np.array_equal(np.unique(a.col), np.arange(a.nU))  # dense U ids
+    assert abs(a.nE - 20000) < 1000
+
+
+def test_batch_spec_ranges(gm):
+    for s in range(1000, 1040):
+        sp = gm.batch_spec(s)
+        assert 50 <= sp.nU <= 5000
+        assert 0.5 * sp.nU - 1 <= sp.nV <= 4 * sp.nU + 1
+        assert 3 * sp.nU - 1 <= sp.n_edges <= 30 * sp.nU + 1
+        assert sp.gamma_u == sp.gamma_v == 2.2
+
+
+def test_adj_roundtrip(gm, tmp_path):
+    g = gm.config_graph("small")
+    p = str(tmp_path / "g.adj")
+    gm.write_adj(p, g)
+    h = gm.read_adj(p)
+    assert np.array_equal(g.row_off, h.row_off) and np.array_equal(g.col, h.col)
+    assert h.nU == g.nU
+    lines = open(p).read().split("\n")
+    assert lines[-1] == "" and all(lines[:-1])
+
+
+@pytest.mark.parametrize("text,code", [
+    ("1 2 3\n3 2\n", "MBE_ERR_FORMAT"),      # row not ascending
+    ("1 2 3\n\n4\n", "MBE_ERR_FORMAT"),      # empty row
+    ("1 1\n", "MBE_ERR_FORMAT"),             # duplicate id
+    ("1 2 x\n", "MBE_ERR_FORMAT"),           # bad token
+    ("1 99999999999\n", "MBE_ERR_FORMAT"),   # id >= 2^31
+])
+def test_adj_rejects_bad_input(gm, tmp_path, text, code):
+    p = tmp_path / "bad.adj"
+    p.write_text(text)
+    with pytest.raises(gm.MBEError) as ei:
+        gm.Graph.from_adj(str(p))
+    assert ei.value.name == code
+
+
+def test_missing_file_is_io_error(gm, tmp_path):
+    with pytest.raises(gm.MBEError) as ei:
+        gm.Graph.from_adj(str(tmp_path / "nope.adj"))
+    assert ei.value.name == "MBE_ERR_IO"
+
+
+def test_truncated_file_reads_partial_last_line(gm, tmp_path):
+    p = tmp_path / "t.adj"
+    p.write_text("0 1\n1 2")  # no trailing newline: still two rows
+    g = gm.read_adj(str(p))
+    assert g.nV == 2 and g.nE == 4
+
+
+def test_csr_validation_runs_before_any_device_call(gm):
+    ro = np.array([0, 2, 2], np.int32)  # second row empty
+    co = np.array([0, 1], np.int32)
+    with pytest.raises(gm.MBEError) as ei:
+        gm.Graph.from_csr(ro, co, 2)
+    assert ei.value.name == "MBE_ERR_FORMAT"
+
+
+def test_params_defaults(gm):
+    p = gm.default_params()
+    assert (p.bound_height, p.bound_size, p.prune) == (20, 1500, 1)

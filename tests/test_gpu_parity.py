@@ -1,0 +1,132 @@
+"""GPU parity: the engine (through the C ABI) against the CPU oracle.
+
+The bar is bit-exact equality of the maximal-biclique count and of the
+canonical set hash.  Oracle sizes are kept to seconds.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from util import planted, random_bipartite
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gm():
+    import gmbe_b200
+    return gmbe_b200
+
+
+def run(gm, ro, co, nU, opts=None, **params):
+    opts = opts or {}
+    with gm.Graph.from_csr(ro, co, nU, **opts) as g:
+        return g.enumerate(**params)
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("shape", [(12, 10, 0.4), (30, 40, 0.25), (40, 60, 0.15), (64, 48, 0.3)])
+def test_tiny_vs_brute_force(gm, seed, shape):
+    nV, nU, p = shape
+    ro, co, nU = random_bipartite(nV, nU, p, seed)
+    bf = oracle.brute_force(ro, co, nU)
+    r = run(gm, ro, co, nU)
+    assert (r.count, r.set_hash) == (bf.count, bf.set_hash)
+
+
+@pytest.mark.parametrize("bitmap", [-1, 32, 64, 0])
+@pytest.mark.parametrize("prune", [1, 0])
+@pytest.mark.parametrize("split", [(20, 1500), (1, 1), (1 << 30, 1 << 30)])
+def test_params_do_not_change_result(gm, bitmap, prune, split):
+    ro, co, nU = planted(300, 200, blocks=6, seed=3, bsize=14)
+    want = oracle.gmbe(ro, co, nU)
+    r = run(gm, ro, co, nU, bitmap_max_l=bitmap, prune=prune, bound_height=split[0],
+            bound_size=split[1])
+    assert r.status == 0
+    assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+@pytest.mark.parametrize("uvtrans,order", [(0, 0), (0, 1), (0, 2), (1, 1), (2, 2), (1, 3)])
+def test_side_swap_and_order(gm, uvtrans, order):
+    ro, co, nU = planted(200, 150, blocks=4, seed=11)
+    want = oracle.brute_force(ro, co, nU) if nU <= 64 else oracle.mbea(ro, co, nU)
+    r = run(gm, ro, co, nU, opts=dict(uvtrans=uvtrans, order=order, fast_mode=int(order != 3)))
+    assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+def test_small_config(gm):
+    g = gm.config_graph("small")
+    want = oracle.gmbe(g.row_off, g.col, g.nU)
+    for uvtrans in (0, 1):
+        r = run(gm, g.row_off, g.col, g.nU, opts=dict(uvtrans=uvtrans))
+        assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+def test_wide_l_uses_counts_tier(gm):
+    # Roots with |L| well above the bitmap limit (128) exercise tier 1 and
+    # its hand-off to tier 2.
+    ro, co, nU = planted(400, 600, blocks=3, seed=5, p_bg=0.3, p_blk=0.9, bsize=20)
+    want = oracle.gmbe(ro, co, nU)
+    for bitmap in (-1, 0):
+        r = run(gm, ro, co, nU, bitmap_max_l=bitmap, bound_height=1 << 30, bound_size=1 << 30)
+        assert (r.count, r.set_hash) == (want.count, want.set_hash)
+        r = run(gm, ro, co, nU, bitmap_max_l=bitmap)
+        assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+def test_root_ranges_add_up(gm):
+    g = gm.config_graph("small")
+    with gm.Graph.from_csr(g.row_off, g.col, g.nU, uvtrans=1) as G:
+        nV = G.info().V_size
+        cuts = [0, nV // 3, nV // 2, nV]
+        tot_c, tot_h = 0, 0
+        for a, b in zip(cuts, cuts[1:]):
+            r = G.enumerate(root_begin=a, root_end=b)
+            o = oracle.gmbe_range(g.row_off, g.col, g.nU, a, b, uvtrans=1)
+            assert (r.count, r.set_hash) == (o.count, o.set_hash)
+            tot_c += r.count
+            tot_h = (tot_h + r.set_hash) % (1 << 64)
+        full = G.enumerate()
+        assert (full.count, full.set_hash) == (tot_c, tot_h)
+
+
+def test_tiny_queue_falls_back_inline(gm):
+    ro, co, nU = planted(300, 200, blocks=6, seed=9, bsize=14)
+    want = oracle.gmbe(ro, co, nU)
+    r = run(gm, ro, co, nU, bound_height=1, bound_size=1, queue_capacity=8)
+    assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+def test_repeat_calls_identical(gm):
+    g = gm.config_graph("small")
+    with gm.Graph.from_csr(g.row_off, g.col, g.nU) as G:
+        a = G.enumerate()
+        b = G.enumerate(blocks=7)
+        c = G.enumerate()
+    assert (a.count, a.set_hash) == (b.count, b.set_hash) == (c.count, c.set_hash)
+
+
+def test_idle_wait_limit_reports_timeout_then_recovers(gm):
+    # One heavy root (a dense block) and many trivial ones: the other warps
+    # run out of work while the heavy root is still pending and give up after
+    # the (tiny) idle limit.  The call must return MBE_ERR_TIMEOUT, not hang,
+    # and the next call on the same graph must be exact.
+    rng = np.random.default_rng(0)
+    rows = []
+    blk = rng.random((22, 22)) < 0.7
+    for i in range(22):
+        r = np.nonzero(blk[i])[0]
+        rows.append(r if len(r) else np.array([0]))
+    for i in range(3000):
+        rows.append(np.array([22 + i]))
+    ro = np.zeros(len(rows) + 1, np.int32)
+    ro[1:] = np.cumsum([len(r) for r in rows])
+    co = np.concatenate(rows).astype(np.int32)
+    nU = int(co.max()) + 1
+    want = oracle.gmbe(ro, co, nU)
+    with gm.Graph.from_csr(ro, co, nU) as G:
+        with pytest.raises(gm.MBEError) as ei:
+            G.enumerate(wait_limit_ns=1, blocks=1, bound_height=1 << 30, bound_size=1 << 30)
+        assert ei.value.name == "MBE_ERR_TIMEOUT"
+        r = G.enumerate()
+        assert (r.count, r.set_hash) == (want.count, want.set_hash)
