@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Benchmark: maximal-biclique enumeration of the medium skewed workload.
+
+One step = one complete enumeration of the medium graph (100k x 400k Chung-Lu,
+~2M edges, 64 planted 24x24 blocks; seeded, synthetic) through the engine,
+with the reference's flags -t 1 -o 1 -f and bounds 20/1500.  The graph is
+resident in HBM before the timed region; every step's count and set hash are
+checked against the recorded oracle values.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: each rank enumerates an interleaved share of the
+roots (shard_index = rank) and one NCCL all-reduce sums (count, set hash) per
+step; value = the graph's bicliques / the slowest rank's device time.
+
+--impl reference times the CPU restatement of the same path (oracle/, the
+GMBE per-root DFS with OpenMP over every host core) on a stratified sample of
+the roots, because the reference has no CPU implementation of its GPU path.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+WORKLOAD = "medium"
+METRIC = "maximal bicliques/s"
+UNIT = "bicliques/s"
+FLAGS = dict(uvtrans=1, order=1, fast_mode=1)
+CONSTS = os.path.join(ROOT, "gmbe_b200", "workload_constants.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def load_consts():
+    with open(CONSTS) as f:
+        return json.load(f)[WORKLOAD]
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax.append(float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(g, target_s=10.0):
+    """Oracle (CPU port of the path, all host cores) on a stratified root
+    sample sized to ~target_s; returns (bicliques/s, description, cores)."""
+    import oracle
+    cores = os.cpu_count() or 1
+    t = time.perf_counter()
+    oracle.gmbe_strided(g.row_off, g.col, g.nU, 1 << 30, 1, threads=cores)  # graph set-up only
+    t_setup = time.perf_counter() - t
+    stride = 512
+    while True:
+        t = time.perf_counter()
+        r = oracle.gmbe_strided(g.row_off, g.col, g.nU, 0, stride, threads=cores)
+        dt = max(time.perf_counter() - t - t_setup, 1e-6)
+        if dt >= target_s / 4 or stride == 1:
+            break
+        stride = max(1, stride // 4)
+    return r.count / dt, f"every {stride}th root of the {WORKLOAD} graph from the top of the " \
+                         f"degree order: {r.count} bicliques in {dt:.2f} s (graph set-up excluded)", cores
+
+
+def run_reference(args):
+    """The reference arm: CPU restatement of the path on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import gmbe_b200 as gm
+    import oracle
+    g = gm.config_graph(WORKLOAD)
+    cores = os.cpu_count() or 1
+    t = time.perf_counter()
+    oracle.gmbe_strided(g.row_off, g.col, g.nU, 1 << 30, 1, threads=cores)
+    t_setup = time.perf_counter() - t
+    # Sample size: ~20 s for the whole run.
+    stride = 256
+    t = time.perf_counter()
+    oracle.gmbe_strided(g.row_off, g.col, g.nU, 0, stride, threads=cores)
+    per = max(time.perf_counter() - t - t_setup, 1e-3)
+    budget = 20.0 / max(1, args.steps + args.warmup)
+    while per * 2 < budget and stride > 1:
+        stride //= 2
+        per *= 2
+    for i in range(args.warmup):
+        oracle.gmbe_strided(g.row_off, g.col, g.nU, i % stride, stride, threads=cores)
+    tot, cnt = 0.0, 0
+    for i in range(args.steps):
+        t = time.perf_counter()
+        r = oracle.gmbe_strided(g.row_off, g.col, g.nU, i % stride, stride, threads=cores)
+        tot += max(time.perf_counter() - t - t_setup, 1e-9)
+        cnt += r.count
+    value = cnt / tot
+    sample = (f"per step every {stride}th root of the {WORKLOAD} graph (offsets 0..{args.steps - 1}), "
+              f"CPU restatement of the GMBE path, OpenMP over roots; graph set-up excluded")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": {"workload": WORKLOAD_DESC(), "flags": "-t 1 -o 1 -f",
+                                        "bound_height": 20, "bound_size": 1500},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def WORKLOAD_DESC():
+    import gmbe_b200 as gm
+    return gm.DESCRIPTIONS[WORKLOAD]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gmbe_b200 as gm
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    consts = load_consts()
+    g = gm.config_graph(WORKLOAD)
+    G = gm.Graph.from_csr(g.row_off, g.col, g.nU, device=local, **FLAGS)
+    shard = dict(shard_count=world, shard_index=rank) if world > 1 else {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def reduce_result(r):
+        t = torch.tensor([int(np.int64(np.uint64(r.count))), int(np.uint64(r.set_hash).view(np.int64))],
+                         dtype=torch.int64, device=dev)
+        if world > 1:
+            dist.all_reduce(t)
+        c, h = t.tolist()
+        return int(np.int64(c).view(np.uint64)), int(np.int64(h).view(np.uint64))
+
+    def check(c, h):
+        if (c, h) != (consts["count"], int(consts["set_hash"], 16)):
+            raise SystemExit(f"result mismatch: count {c} hash {h:#x}, expected "
+                             f"{consts['count']} {consts['set_hash']}")
+
+    for _ in range(args.warmup):
+        check(*reduce_result(G.enumerate(**shard)))
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    step_ms, kern_ms, exit_skew = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier()
+        ev0.record()
+        r = G.enumerate(sm_timing=1, **shard)
+        ev1.record()
+        torch.cuda.synchronize()
+        barrier()
+        step_ms.append(ev0.elapsed_time(ev1))
+        kern_ms.append(r.kernel_ms)
+        exit_skew.append(r.sm_exit_max_ms - r.sm_exit_min_ms)
+        check(*reduce_result(r))
+    clk = clocks.stop()
+    total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
+    kern_total = torch.tensor([sum(kern_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(total_ms, op=dist.ReduceOp.MAX)
+        dist.all_reduce(kern_total, op=dist.ReduceOp.MAX)
+    total_ms = float(total_ms.item())
+    kern_mean_ms = float(kern_total.item()) / args.steps
+    value = consts["count"] * args.steps / (total_ms / 1000.0)
+
+    # ---- end to end through the public API with host buffers ----
+    e2e_steps = max(1, min(args.steps, 3))
+    # CSR, its transpose and the per-vertex hash keys are uploaded per call.
+    h2d = 4 * ((g.nV + 1) + (g.nU + 1) + 2 * g.nE) + 8 * (g.nV + g.nU)
+    d2h = 152  # the result block read back per call
+    e2e_s = []
+    G.free()
+    for _ in range(e2e_steps):
+        barrier()
+        t = time.perf_counter()
+        with gm.Graph.from_csr(g.row_off, g.col, g.nU, device=local, **FLAGS) as G2:
+            r = G2.enumerate(**shard)
+        e2e_s.append(time.perf_counter() - t)
+        check(*reduce_result(r))
+    e2e_tot = torch.tensor([sum(e2e_s)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+    e2e_value = consts["count"] * e2e_steps / float(e2e_tot.item())
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        alg = consts["alg_bytes"] / max(world, 1)
+        achieved = alg / (kern_mean_ms / 1000.0) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC(), "flags": "-t 1 -o 1 -f", "bound_height": 20,
+                       "bound_size": 1500, "bicliques_per_step": consts["count"],
+                       "parallelism": f"roots interleaved over {world} GPU(s)" if world > 1 else "1 GPU",
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "enum_ms_per_step": kern_mean_ms,
+            "sm_exit_skew_ms": statistics.median(exit_skew),
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": consts.get("traffic_bytes_per_launch"),
+                         "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg,
+                         "kernel": "mbe_enum_kernel"},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            v, sample, cores = cpu_sample(g)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                    "sample": sample}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

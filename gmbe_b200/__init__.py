@@ -56,7 +56,7 @@ class Params(C.Structure):
                 ("blocks", C.c_int32), ("queue_capacity", C.c_int32),
                 ("bitmap_max_l", C.c_int32), ("wait_limit_ns", C.c_int64),
                 ("sm_timing", C.c_int32), ("root_begin", C.c_int32), ("root_end", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("shard_count", C.c_int32), ("shard_index", C.c_int32)]
 
 
 class Result(C.Structure):

@@ -23,16 +23,6 @@ struct mbe_graph {
   int32_t* d_rev_col = nullptr;
   uint64_t* d_ukey = nullptr;
   uint64_t* d_vkey = nullptr;
-  // Cached engine workspace (grown on demand, reused across enumerations).
-  int32_t* d_scratch = nullptr;
-  size_t scratch_bytes = 0;
-  EnumCtl* d_ctl = nullptr;
-  Task* d_q_tasks = nullptr;
-  unsigned long long* d_q_seq = nullptr;
-  int32_t q_cap = 0;
-  unsigned long long* d_exit = nullptr;
-  int32_t exit_cap = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // Capacities derived from the graph (max over roots).
   int32_t capS = 0, capL = 0;
 };
@@ -71,22 +61,31 @@ void free_device(mbe_graph* g) {
   cudaFree(g->d_rev_col);
   cudaFree(g->d_ukey);
   cudaFree(g->d_vkey);
-  cudaFree(g->d_scratch);
-  cudaFree(g->d_ctl);
-  cudaFree(g->d_q_tasks);
-  cudaFree(g->d_q_seq);
-  cudaFree(g->d_exit);
-  if (g->ev0) cudaEventDestroy(g->ev0);
-  if (g->ev1) cudaEventDestroy(g->ev1);
   g->d_row_off = g->d_col = g->d_rev_off = g->d_rev_col = nullptr;
   g->d_ukey = g->d_vkey = nullptr;
-  g->d_scratch = nullptr;
-  g->d_ctl = nullptr;
-  g->d_q_tasks = nullptr;
-  g->d_q_seq = nullptr;
-  g->d_exit = nullptr;
-  g->ev0 = g->ev1 = nullptr;
 }
+
+// Engine workspace, one per device, shared by every graph on that device
+// and reused across calls (grown on demand).  A call holds the device's
+// workspace for its whole duration.
+struct Workspace {
+  std::mutex mu;
+  int32_t* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  EnumCtl* ctl = nullptr;
+  Task* q_tasks = nullptr;
+  unsigned long long* q_seq = nullptr;
+  int32_t q_cap = 0;
+  unsigned long long* exit_ns = nullptr;
+  int32_t exit_cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Layout the per-warp count maps were last cleared for.
+  int64_t map_pitch_words = -1, map_words = -1;
+  int32_t map_warps = -1;
+};
+
+constexpr int kMaxDevices = 64;
+Workspace g_ws[kMaxDevices];
 
 template <typename T>
 int upload(T** dst, const std::vector<T>& src) {
@@ -127,8 +126,6 @@ int upload_graph(mbe_graph* g) {
   if (capS > INT32_MAX / 2) return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
   g->capS = (int32_t)std::max<int64_t>(capS, 1);
   g->capL = std::max(capL, 1);
-  CK(cudaEventCreate(&g->ev0));
-  CK(cudaEventCreate(&g->ev1));
   return MBE_OK;
 }
 
@@ -271,17 +268,29 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   if (params) prm = *params;
   else mbe_params_default(&prm);
   const double t0 = now_s();  // reference exe_time_ starts at Execute() (src/IterFinderGpu.cu:1096)
+  if (g->device < 0 || g->device >= kMaxDevices) return set_error(MBE_ERR_INVALID, "bad device");
   CK(cudaSetDevice(g->device));
   const HostGraph& h = g->h;
   int32_t rb = prm.root_begin, re = prm.root_end;
   if (rb == 0 && re == 0) re = h.V_size;
   if (rb < 0 || re > h.V_size || rb > re)
     return set_error(MBE_ERR_INVALID, "root range [%d,%d) outside [0,%d)", rb, re, h.V_size);
+  int32_t sc = prm.shard_count > 1 ? prm.shard_count : 1;
+  int32_t si = prm.shard_count > 1 ? prm.shard_index : 0;
+  if (si < 0 || si >= sc) return set_error(MBE_ERR_INVALID, "shard_index %d outside [0,%d)", si, sc);
+  int32_t span = re - rb;
+  int32_t n_roots = span > si ? (span - si + sc - 1) / sc : 0;
   int t2 = prm.bitmap_max_l;
   if (t2 == 0) t2 = 32 * kKMax;
   if (t2 < 0) t2 = 1;
   if (t2 > 32 * kKMax) return set_error(MBE_ERR_INVALID, "bitmap_max_l > %d", 32 * kKMax);
 
+  Workspace& ws = g_ws[g->device];
+  std::lock_guard<std::mutex> lock(ws.mu);
+  if (!ws.ev0) {
+    CK(cudaEventCreate(&ws.ev0));
+    CK(cudaEventCreate(&ws.ev1));
+  }
   // ---- launch shape and workspace ----
   int dev_sms = 0;
   CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device));
@@ -293,36 +302,48 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   int32_t capC = std::max<int32_t>(1, std::min<int32_t>(h.V_size, g->capS));
   ScratchLayout sl = make_layout(h.V_size, capC, g->capL, g->capS);
   size_t need = (size_t)sl.words_per_warp * (size_t)warps * sizeof(int32_t);
-  if (need > g->scratch_bytes) {
-    cudaFree(g->d_scratch);
-    g->d_scratch = nullptr;
-    g->scratch_bytes = 0;
-    cudaError_t e = cudaMalloc((void**)&g->d_scratch, need);
+  if (need > ws.scratch_bytes) {
+    cudaFree(ws.scratch);
+    ws.scratch = nullptr;
+    ws.scratch_bytes = 0;
+    cudaError_t e = cudaMalloc((void**)&ws.scratch, need);
     if (e != cudaSuccess)
       return set_error(MBE_ERR_NOMEM, "scratch of %.2f GB: %s", need / 1e9, cudaGetErrorString(e));
-    g->scratch_bytes = need;
-    CK(cudaMemset(g->d_scratch, 0, need));  // the dense count maps start (and end) at zero
+    ws.scratch_bytes = need;
+    ws.map_pitch_words = -1;
+  }
+  // Every task leaves its warp's dense count map all-zero.  A different
+  // layout puts the maps elsewhere: clear them (strided, maps only).
+  if (ws.map_pitch_words != sl.words_per_warp || ws.map_words != h.V_size || ws.map_warps < warps) {
+    CK(cudaMemset2DAsync(ws.scratch, (size_t)sl.words_per_warp * sizeof(int32_t), 0,
+                         (size_t)std::max<int32_t>(h.V_size, 1) * sizeof(int32_t), (size_t)warps));
+    ws.map_pitch_words = sl.words_per_warp;
+    ws.map_words = h.V_size;
+    ws.map_warps = warps;
   }
   int32_t qcap = prm.queue_capacity > 0
                      ? prm.queue_capacity
                      : (int32_t)std::min<int64_t>(1 << 22, std::max<int64_t>(1 << 16, 8LL * h.V_size));
-  if (qcap != g->q_cap) {
-    cudaFree(g->d_q_tasks);
-    cudaFree(g->d_q_seq);
-    g->d_q_tasks = nullptr;
-    g->d_q_seq = nullptr;
-    CK(cudaMalloc((void**)&g->d_q_tasks, sizeof(Task) * (size_t)qcap));
-    CK(cudaMalloc((void**)&g->d_q_seq, sizeof(unsigned long long) * (size_t)qcap));
-    g->q_cap = qcap;
+  if (qcap != ws.q_cap) {
+    cudaFree(ws.q_tasks);
+    cudaFree(ws.q_seq);
+    ws.q_tasks = nullptr;
+    ws.q_seq = nullptr;
+    ws.q_cap = 0;
+    CK(cudaMalloc((void**)&ws.q_tasks, sizeof(Task) * (size_t)qcap));
+    CK(cudaMalloc((void**)&ws.q_seq, sizeof(unsigned long long) * (size_t)qcap));
+    ws.q_cap = qcap;
   }
-  if (!g->d_ctl) CK(cudaMalloc((void**)&g->d_ctl, sizeof(EnumCtl)));
-  if (blocks > g->exit_cap) {
-    cudaFree(g->d_exit);
-    CK(cudaMalloc((void**)&g->d_exit, sizeof(unsigned long long) * (size_t)blocks));
-    g->exit_cap = blocks;
+  if (!ws.ctl) CK(cudaMalloc((void**)&ws.ctl, sizeof(EnumCtl)));
+  if (blocks > ws.exit_cap) {
+    cudaFree(ws.exit_ns);
+    ws.exit_ns = nullptr;
+    ws.exit_cap = 0;
+    CK(cudaMalloc((void**)&ws.exit_ns, sizeof(unsigned long long) * (size_t)blocks));
+    ws.exit_cap = blocks;
   }
-  CK(cudaMemsetAsync(g->d_ctl, 0, sizeof(EnumCtl)));
-  CK(cudaMemsetAsync(g->d_q_seq, 0, sizeof(unsigned long long) * (size_t)qcap));
+  CK(cudaMemsetAsync(ws.ctl, 0, sizeof(EnumCtl)));
+  CK(cudaMemsetAsync(ws.q_seq, 0, sizeof(unsigned long long) * (size_t)qcap));
 
   DevGraph dg;
   dg.nV = h.V_size;
@@ -335,8 +356,10 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   dg.ukey = g->d_ukey;
   dg.vkey = g->d_vkey;
   dg.swapped = h.swapped;
-  dg.root_begin = rb;
   dg.root_end = re;
+  dg.root_offset = si;
+  dg.root_stride = sc;
+  dg.n_roots = n_roots;
   EnumParams ep;
   memset(&ep, 0, sizeof(ep));
   ep.bound_height = prm.bound_height;
@@ -348,15 +371,15 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   ep.record_exit = prm.sm_timing ? 1 : 0;
   ep.tier2_max_l = t2;
 
-  CK(cudaEventRecord(g->ev0));
-  mbe_enum_kernel<<<blocks, kEnumThreads>>>(dg, ep, sl, g->d_ctl, g->d_q_tasks, g->d_q_seq,
-                                            g->d_scratch, g->d_exit);
+  CK(cudaEventRecord(ws.ev0));
+  mbe_enum_kernel<<<blocks, kEnumThreads>>>(dg, ep, sl, ws.ctl, ws.q_tasks, ws.q_seq, ws.scratch,
+                                            ws.exit_ns);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(g->ev1));
+  CK(cudaEventRecord(ws.ev1));
   EnumCtl ctl;
-  CK(cudaMemcpy(&ctl, g->d_ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&ctl, ws.ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost));
   float ms = 0;
-  CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+  CK(cudaEventElapsedTime(&ms, ws.ev0, ws.ev1));
   out->count = ctl.count;
   out->set_hash = ctl.hash;
   out->non_maximal = ctl.non_maximal;
@@ -365,7 +388,7 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   out->status = ctl.status;
   if (prm.sm_timing) {
     std::vector<unsigned long long> ex(blocks);
-    CK(cudaMemcpy(ex.data(), g->d_exit, sizeof(unsigned long long) * blocks, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ex.data(), ws.exit_ns, sizeof(unsigned long long) * blocks, cudaMemcpyDeviceToHost));
     auto mm = std::minmax_element(ex.begin(), ex.end());
     out->sm_exit_min_ms = *mm.first / 1e6;
     out->sm_exit_max_ms = *mm.second / 1e6;
@@ -373,7 +396,7 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   out->enum_seconds = now_s() - t0;
   if (ctl.status != 0) {
     // An aborted run leaves count maps dirty: clear them for the next call.
-    cudaMemset(g->d_scratch, 0, g->scratch_bytes);
+    ws.map_pitch_words = -1;
     switch (ctl.status) {
       case kStTimeout:
         return set_error(MBE_ERR_TIMEOUT, "device wait limit reached (idle %llu ns)", ctl.err_info);

@@ -24,7 +24,9 @@ struct DevGraph {
   const uint64_t* ukey;    // [nU] hash key of internal U vertex (original id, original side)
   const uint64_t* vkey;    // [nV]
   int32_t swapped;         // internal U is the original V side
-  int32_t root_begin, root_end;  // roots [root_begin, root_end) are enumerated
+  // Roots: position p = 0 .. n_roots-1 is internal vertex
+  // root_end - 1 - (root_offset + p * root_stride).
+  int32_t root_end, root_offset, root_stride, n_roots;
 };
 
 // A task: up to four internal V vertices, -1 padded (reference LongTask,

@@ -801,9 +801,19 @@ __device__ void run_task(Warp& W, const Task& t) {
           if (trivially) continue;
           const int32_t* rw = g.col + g.row_off[ww];
           int dw = g.row_off[ww + 1] - g.row_off[ww];
+          // ww covers L_parent only if it has at least |L_parent| neighbours;
+          // otherwise it is a new R vertex below `last`: not maximal here.
+          if (dw < nLp) {
+            ism = false;
+            break;
+          }
           bool all = true;
-          for (int j = lane; j < nLp; j += 32) all &= contains_sorted(rw, dw, Lpar[j]);
-          if (!__all_sync(kFull, all)) ism = false;
+          for (int j0 = 0; j0 < nLp && all; j0 += 32) {
+            int j = j0 + lane;
+            bool in = j >= nLp || contains_sorted(rw, dw, Lpar[j]);
+            all = __all_sync(kFull, in);
+          }
+          if (!all) ism = false;
         }
       }
     }
@@ -947,7 +957,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   W.q_seq = q_seq;
   W.base = scratch + (size_t)warp_global * (size_t)sl.words_per_warp;
   W.cnt = W.hash = W.nonmax = W.splits = 0;
-  const int nroots = g.root_end - g.root_begin;
+  const int nroots = g.n_roots;
   uint64_t idle_since = 0;
   while (true) {
     int ab = lane == 0 ? *(volatile int32_t*)&ctl->abort : 0;
@@ -960,7 +970,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
         atomicAdd(&ctl->pending, 1ULL);
         int r = atomicAdd(&ctl->next_root, 1);
         if (r < nroots) {
-          t.v[0] = g.root_end - 1 - r;
+          t.v[0] = g.root_end - 1 - (g.root_offset + r * g.root_stride);
           t.v[1] = t.v[2] = t.v[3] = -1;
           have = 1;
         } else {

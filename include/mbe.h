@@ -86,7 +86,8 @@ typedef struct mbe_params {
   int32_t sm_timing;       /* -p: record each block's exit time */
   int32_t root_begin;      /* enumerate only roots [root_begin, root_end) of the internal */
   int32_t root_end;        /*   order (0, 0 = all); the internal order is -t/-o applied   */
-  int32_t reserved;
+  int32_t shard_count;     /* 0/1 = every root of the range; n > 1 = only the roots at     */
+  int32_t shard_index;     /*   positions p = shard_index mod n, counted from the top      */
 } mbe_params;
 
 typedef struct mbe_result {

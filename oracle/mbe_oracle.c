@@ -561,6 +561,58 @@ int orc_gmbe_range(int32_t nV, int32_t nU, const int32_t* row_off, const int32_t
   return 0;
 }
 
+/* Stratified sample: roots at positions p = offset, offset+stride, ... counted
+ * from the top of the internal order (the reference claims roots from
+ * V_size-1 downwards, src/IterFinderGpu.cu:1008).  Used to time a bounded
+ * share of a workload whose degree-sorted roots vary widely in cost. */
+int orc_gmbe_strided(int32_t nV, int32_t nU, const int32_t* row_off, const int32_t* col,
+                     int32_t uvtrans, int32_t order, int32_t prune, int32_t threads,
+                     int64_t offset, int64_t stride, orc_result* out) {
+  memset(out, 0, sizeof(*out));
+  if (stride < 1 || offset < 0) return -1;
+  ograph g;
+  ograph_build(nV, nU, row_off, col, uvtrans, order, &g);
+  int32_t maxdv = 0;
+  for (int32_t v = 0; v < g.nV; ++v) if (deg_v(&g, v) > maxdv) maxdv = (int32_t)deg_v(&g, v);
+  if (threads <= 0) threads = omp_get_max_threads();
+  int64_t n = g.nV > offset ? (g.nV - offset + stride - 1) / stride : 0;
+  uint64_t cnt = 0, hash = 0, nonmax = 0, bytes = 0, nodes = 0;
+#pragma omp parallel num_threads(threads) reduction(+ : cnt, hash, nonmax, bytes, nodes)
+  {
+    gws w;
+    size_t nv = (size_t)(g.nV > 0 ? g.nV : 1);
+    w.cnt = (int32_t*)calloc(nv, sizeof(int32_t));
+    w.posC = (int32_t*)malloc(nv * sizeof(int32_t));
+    for (size_t i = 0; i < nv; ++i) w.posC[i] = -1;
+    w.touched = (int32_t*)malloc(nv * sizeof(int32_t));
+    w.Cv = (int32_t*)malloc(nv * sizeof(int32_t));
+    w.ncnt = (int32_t*)malloc(nv * sizeof(int32_t));
+    w.bound = (int32_t*)malloc(nv * sizeof(int32_t));
+    w.stack = (int32_t*)malloc((nv + 2) * sizeof(int32_t));
+    w.Llevel = (int32_t*)malloc(((size_t)maxdv + 1) * sizeof(int32_t));
+    w.aoff = (int32_t*)malloc(((size_t)maxdv + 2) * sizeof(int32_t));
+    w.aadj_cap = 1 << 16;
+    w.aadj = (int32_t*)malloc(w.aadj_cap * sizeof(int32_t));
+    gacc a = {0, 0, 0, 0, 0};
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t k = 0; k < n; ++k) gmbe_root(&g, (int32_t)(g.nV - 1 - (offset + k * stride)), prune, &w, &a, NULL);
+    cnt += a.count;
+    hash += a.hash;
+    nonmax += a.non_max;
+    bytes += a.bytes;
+    nodes += a.nodes;
+    free(w.cnt); free(w.posC); free(w.touched); free(w.Cv); free(w.ncnt); free(w.bound);
+    free(w.stack); free(w.Llevel); free(w.aoff); free(w.aadj);
+  }
+  out->count = cnt;
+  out->set_hash = hash;
+  out->non_maximal = nonmax;
+  out->alg_bytes = bytes;
+  out->nodes = nodes;
+  ograph_free(&g);
+  return 0;
+}
+
 int orc_gmbe(int32_t nV, int32_t nU, const int32_t* row_off, const int32_t* col, int32_t uvtrans,
              int32_t order, int32_t prune, int32_t threads, orc_result* out) {
   return orc_gmbe_range(nV, nU, row_off, col, uvtrans, order, prune, threads, 0, 0, NULL, out);

@@ -36,6 +36,8 @@ def _load():
     lib.orc_gmbe_range.argtypes = [C.c_int32, C.c_int32, P32, P32, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, C.c_int64, C.c_int64,
                                    C.POINTER(C.c_int64), C.c_void_p]
+    lib.orc_gmbe_strided.argtypes = [C.c_int32, C.c_int32, P32, P32, C.c_int32, C.c_int32,
+                                     C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_void_p]
     lib.orc_internal_order.argtypes = [C.c_int32, C.c_int32, P32, P32, C.c_int32, C.c_int32,
                                        P32, P32]
     return lib
@@ -103,6 +105,16 @@ def gmbe_range(row_off, col, nU, root_begin, root_end, uvtrans=1, order=1, prune
     lib().orc_gmbe_range(len(ro) - 1, nU, pr, pc, uvtrans, order, prune, threads,
                          root_begin, root_end, stp, C.byref(r))
     return (r, st) if stats else r
+
+
+def gmbe_strided(row_off, col, nU, offset, stride, uvtrans=1, order=1, prune=1, threads=0):
+    """Roots at positions offset, offset+stride, ... from the top of the
+    internal order (a stratified sample of a degree-sorted root list)."""
+    ro, co, pr, pc = _arrs(row_off, col)
+    r = OrcResult()
+    lib().orc_gmbe_strided(len(ro) - 1, nU, pr, pc, uvtrans, order, prune, threads, offset,
+                           stride, C.byref(r))
+    return r
 
 
 def ref_binary(name: str) -> str | None:

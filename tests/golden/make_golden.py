@@ -35,6 +35,7 @@ import oracle  # noqa: E402
 from util import planted, random_bipartite  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
+CONSTS = os.path.join(ROOT, "gmbe_b200", "workload_constants.json")
 
 
 def csr_digest(ro, co):
@@ -51,12 +52,15 @@ def run_ref(args, timeout):
     return (int(m.group(1)) if m else None), time.time() - t
 
 
-def case(name, ro, co, nU, ref_timeout=600, uvtrans=1):
+def case(name, ro, co, nU, ref_timeout=600, uvtrans=1, refs_to_run=None):
     entry = {"name": name, "nV": int(len(ro) - 1), "nU": int(nU), "nE": int(len(co)),
              "csr_sha256_16": csr_digest(ro, co)}
+    t = time.time()
     o = oracle.gmbe(ro, co, nU, uvtrans=uvtrans)
+    entry["oracle_seconds"] = round(time.time() - t, 3)
     entry["oracle_count"] = int(o.count)
     entry["oracle_set_hash"] = f"{o.set_hash:#018x}"
+    entry["oracle_alg_bytes"] = int(o.alg_bytes)
     if nU <= 64:
         bf = oracle.brute_force(ro, co, nU)
         entry["brute_force_count"] = int(bf.count)
@@ -67,8 +71,11 @@ def case(name, ro, co, nU, ref_timeout=600, uvtrans=1):
         gm.write_adj(path, gm.BipartiteCSR(np.asarray(ro), np.asarray(co), nU))
         mbea = oracle.ref_binary("ref_mbea")
         mbe = oracle.ref_binary("MBE")
+        want = refs_to_run or ("MbeaFinderBitset", "MbeaFinder", "PMBE", "iMBEA", "MBEA")
         if mbea:
             for sel, label in ((1, "MbeaFinderBitset"), (0, "MbeaFinder")):
+                if label not in want:
+                    continue
                 try:
                     c, t = run_ref([mbea, path, str(sel), str(uvtrans), "1"], ref_timeout)
                     refs[label] = {"count": c, "seconds": round(t, 3)}
@@ -76,6 +83,8 @@ def case(name, ro, co, nU, ref_timeout=600, uvtrans=1):
                     refs[label] = {"count": None, "timeout_s": ref_timeout}
         if mbe:
             for sel, label in ((2, "PMBE"), (1, "iMBEA"), (0, "MBEA")):
+                if label not in want:
+                    continue
                 try:
                     c, t = run_ref([mbe, "-i", path, "-s", str(sel)], ref_timeout)
                     refs[label] = {"count": c, "seconds": round(t, 3)}
@@ -103,7 +112,17 @@ def main():
         cases.append(case(f"batch_{seed}", b.row_off, b.col, b.nU))
     if a.with_medium:
         g = gm.config_graph("medium")
-        cases.append(case("config_medium", g.row_off, g.col, g.nU, ref_timeout=3600))
+        c = case("config_medium", g.row_off, g.col, g.nU, ref_timeout=2400,
+                 refs_to_run=("MbeaFinderBitset", "PMBE"))
+        cases.append(c)
+        consts = {"medium": {"count": c["oracle_count"], "set_hash": c["oracle_set_hash"],
+                             "alg_bytes": c["oracle_alg_bytes"],
+                             "csr_sha256_16": c["csr_sha256_16"],
+                             "flags": "-t 1 -o 1 -f, pruning on",
+                             "source": "tests/golden/make_golden.py --with-medium (CPU oracle)"}}
+        with open(CONSTS, "w") as f:
+            json.dump(consts, f, indent=1)
+        print("wrote", CONSTS)
     with open(OUT, "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "cases": cases}, f, indent=1)
     print("wrote", OUT)

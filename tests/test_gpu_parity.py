@@ -62,16 +62,37 @@ def test_small_config(gm):
         assert (r.count, r.set_hash) == (want.count, want.set_hash)
 
 
-def test_wide_l_uses_counts_tier(gm):
+def hub_graph(seed, nV=600, nU=1200, hubs=10, hub_deg=300, p_bg=0.004):
+    """Sparse background plus a few V rows of degree ~hub_deg (|L| > 128)."""
+    rng = np.random.default_rng(seed)
+    A = rng.random((nV, nU)) < p_bg
+    for h in rng.choice(nV, size=hubs, replace=False):
+        A[h, rng.choice(nU, size=hub_deg, replace=False)] = True
+    for v in range(nV):
+        if not A[v].any():
+            A[v, rng.integers(nU)] = True
+    for u in range(nU):
+        if not A[:, u].any():
+            A[rng.integers(nV), u] = True
+    rows = [np.nonzero(A[v])[0].astype(np.int32) for v in range(nV)]
+    ro = np.zeros(nV + 1, np.int32)
+    ro[1:] = np.cumsum([len(r) for r in rows])
+    return ro, np.concatenate(rows).astype(np.int32), nU
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_wide_l_uses_counts_tier(gm, seed):
     # Roots with |L| well above the bitmap limit (128) exercise tier 1 and
-    # its hand-off to tier 2.
-    ro, co, nU = planted(400, 600, blocks=3, seed=5, p_bg=0.3, p_blk=0.9, bsize=20)
+    # its hand-off to tier 2, with and without splitting.
+    ro, co, nU = hub_graph(seed)
     want = oracle.gmbe(ro, co, nU)
-    for bitmap in (-1, 0):
-        r = run(gm, ro, co, nU, bitmap_max_l=bitmap, bound_height=1 << 30, bound_size=1 << 30)
-        assert (r.count, r.set_hash) == (want.count, want.set_hash)
-        r = run(gm, ro, co, nU, bitmap_max_l=bitmap)
-        assert (r.count, r.set_hash) == (want.count, want.set_hash)
+    for uvtrans in (0, 2):
+        for bitmap in (-1, 0):
+            r = run(gm, ro, co, nU, opts=dict(uvtrans=uvtrans), bitmap_max_l=bitmap,
+                    bound_height=1 << 30, bound_size=1 << 30)
+            assert (r.count, r.set_hash) == (want.count, want.set_hash)
+            r = run(gm, ro, co, nU, opts=dict(uvtrans=uvtrans), bitmap_max_l=bitmap)
+            assert (r.count, r.set_hash) == (want.count, want.set_hash)
 
 
 def test_root_ranges_add_up(gm):
@@ -107,10 +128,11 @@ def test_repeat_calls_identical(gm):
 
 
 def test_idle_wait_limit_reports_timeout_then_recovers(gm):
-    # One heavy root (a dense block) and many trivial ones: the other warps
-    # run out of work while the heavy root is still pending and give up after
-    # the (tiny) idle limit.  The call must return MBE_ERR_TIMEOUT, not hang,
-    # and the next call on the same graph must be exact.
+    # Many trivial roots, then (input order, roots are taken from the last
+    # row backwards) the rows of a dense block: the warps that find no more
+    # roots idle while the block is still pending and give up after the
+    # (tiny) idle limit.  The call must return MBE_ERR_TIMEOUT, not hang, and
+    # the next call on the same graph must be exact.
     rng = np.random.default_rng(0)
     rows = []
     blk = rng.random((22, 22)) < 0.7
@@ -124,7 +146,7 @@ def test_idle_wait_limit_reports_timeout_then_recovers(gm):
     co = np.concatenate(rows).astype(np.int32)
     nU = int(co.max()) + 1
     want = oracle.gmbe(ro, co, nU)
-    with gm.Graph.from_csr(ro, co, nU) as G:
+    with gm.Graph.from_csr(ro, co, nU, order=0) as G:
         with pytest.raises(gm.MBEError) as ei:
             G.enumerate(wait_limit_ns=1, blocks=1, bound_height=1 << 30, bound_size=1 << 30)
         assert ei.value.name == "MBE_ERR_TIMEOUT"
