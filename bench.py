@@ -227,7 +227,7 @@ def main():
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    step_ms, kern_ms, exit_skew = [], [], []
+    step_ms, kern_ms, exit_skew, busy = [], [], [], []
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -240,6 +240,7 @@ def main():
         step_ms.append(ev0.elapsed_time(ev1))
         kern_ms.append(r.kernel_ms)
         exit_skew.append(r.sm_exit_max_ms - r.sm_exit_min_ms)
+        busy.append(r.warp_busy_frac)
         check(*reduce_result(r))
     clk = clocks.stop()
     total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
@@ -283,7 +284,8 @@ def main():
                        "parallelism": f"roots interleaved over {world} GPU(s)" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB write) before every timed step"},
             "enum_ms_per_step": kern_mean_ms,
-            "sm_exit_skew_ms": statistics.median(exit_skew),
+            "sm_last_task_skew_ms": statistics.median(exit_skew),
+            "warp_busy_frac": statistics.median(busy),
             "gpu_launches": args.steps,
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,

@@ -63,7 +63,8 @@ class Result(C.Structure):
     _fields_ = [("count", C.c_uint64), ("set_hash", C.c_uint64), ("non_maximal", C.c_uint64),
                 ("tasks_split", C.c_uint64), ("enum_seconds", C.c_double),
                 ("kernel_ms", C.c_float), ("status", C.c_int32),
-                ("sm_exit_max_ms", C.c_double), ("sm_exit_min_ms", C.c_double)]
+                ("sm_exit_max_ms", C.c_double), ("sm_exit_min_ms", C.c_double),
+                ("warp_busy_frac", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -180,8 +180,16 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   s.lkey = take(2 * T2);
   s.lmask = take((T2 + 2) * kKMax);
   s.cursor2 = take(T2 + 2);
-  s.sr2 = take(2 * (T2 + 2));
-  s.nr2 = take(T2 + 2);
+  s.act_off = take(T2 + 2);
+  s.act_len = take(T2 + 2);
+  s.act_top = take(T2 + 2);
+  s.r_sum = take(2 * (T2 + 2));
+  s.r_cnt = take(T2 + 2);
+  s.tlist = take(C);
+  // Active-list arena of the bitmap tier: the level-1 list plus room for
+  // compacted deeper lists (a level that does not fit shares its parent's).
+  s.act_cap = (int32_t)std::min<int64_t>(INT32_MAX / 2, 3 * C + 4096);
+  s.act = take(s.act_cap);
   s.words_per_warp = off;
   return s;
 }
@@ -339,7 +347,7 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
     cudaFree(ws.exit_ns);
     ws.exit_ns = nullptr;
     ws.exit_cap = 0;
-    CK(cudaMalloc((void**)&ws.exit_ns, sizeof(unsigned long long) * (size_t)blocks));
+    CK(cudaMalloc((void**)&ws.exit_ns, 2 * sizeof(unsigned long long) * (size_t)blocks));
     ws.exit_cap = blocks;
   }
   CK(cudaMemsetAsync(ws.ctl, 0, sizeof(EnumCtl)));
@@ -387,11 +395,15 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   out->kernel_ms = ms;
   out->status = ctl.status;
   if (prm.sm_timing) {
-    std::vector<unsigned long long> ex(blocks);
-    CK(cudaMemcpy(ex.data(), ws.exit_ns, sizeof(unsigned long long) * blocks, cudaMemcpyDeviceToHost));
-    auto mm = std::minmax_element(ex.begin(), ex.end());
+    std::vector<unsigned long long> ex(2 * (size_t)blocks);
+    CK(cudaMemcpy(ex.data(), ws.exit_ns, 2 * sizeof(unsigned long long) * blocks,
+                  cudaMemcpyDeviceToHost));
+    auto mm = std::minmax_element(ex.begin(), ex.begin() + blocks);
     out->sm_exit_min_ms = *mm.first / 1e6;
     out->sm_exit_max_ms = *mm.second / 1e6;
+    double busy = 0;
+    for (int b = 0; b < blocks; ++b) busy += (double)ex[blocks + b];
+    out->warp_busy_frac = ms > 0 ? busy / 1e6 / ((double)warps * ms) : 0.0;
   }
   out->enum_seconds = now_s() - t0;
   if (ctl.status != 0) {

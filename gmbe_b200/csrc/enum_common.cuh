@@ -64,7 +64,9 @@ struct ScratchLayout {
   int64_t lv, llevel, lp, aoff, stack, lsize;
   int64_t aadj, cadj;
   int64_t masks, sub_v, bound2;
-  int64_t lkey, lmask, cursor2, sr2, nr2;  // lkey/sr2 are uint64 (8-byte aligned offsets)
+  int64_t lkey, lmask, cursor2;  // lkey is uint64 (8-byte aligned offset)
+  int64_t act, act_off, act_len, act_top, tlist, r_sum, r_cnt;  // r_sum is uint64
+  int32_t act_cap, pad;
 };
 
 struct EnumParams {

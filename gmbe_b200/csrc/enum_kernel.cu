@@ -93,7 +93,11 @@ struct Warp {
 //   masks[w*capC + i] : word w of candidate i's neighbourhood inside L
 //   subkey[i]         : hash key of candidate i
 //   candidates [0, nq) are Q (already excluded), [nq, nsub) are P.
-// Restates IterProcess / finder_push / finder_pop on bitmaps.
+// Restates IterProcess / finder_push / finder_pop on bitmaps.  Each level
+// keeps an active list: the candidates that still meet the level's L and are
+// not yet absorbed or pruned (MBEA's shrinking P and Q), so deep levels scan
+// only what can still matter.  A level whose list does not fit the arena
+// shares its parent's list (a superset; the scans re-test the mask).
 template <int K>
 __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
   const int lane = (int)lane_id();
@@ -103,12 +107,29 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
   int32_t* bound = W.A(W.sl.bound2);
   const uint64_t* lkey = W.A64(W.sl.lkey);
   uint32_t* lmask = reinterpret_cast<uint32_t*>(W.A(W.sl.lmask));
-  int32_t* cursor = W.A(W.sl.cursor2);
+  int32_t* cursor = W.A(W.sl.cursor2);   // position inside the level's active list
+  int32_t* aoff = W.A(W.sl.act_off);     // level list start in the arena
+  int32_t* alen = W.A(W.sl.act_len);     // level list length
+  int32_t* atop = W.A(W.sl.act_top);     // first free arena word after the level
+  int32_t* act = W.A(W.sl.act);
+  const int actcap = W.sl.act_cap;
   const bool prune = W.p.prune != 0;
+  // R of the push that opened each level: candidates absorbed above a level
+  // are not in its list but still belong to every R below it.
+  uint64_t* rsum = W.A64(W.sl.r_sum);
+  uint32_t* rcnt = reinterpret_cast<uint32_t*>(W.A(W.sl.r_cnt));
 
-  for (int i = lane; i < nsub; i += 32) bound[i] = kFree;
+  for (int i = lane; i < nsub; i += 32) {
+    bound[i] = kFree;
+    act[i] = i;
+  }
   if (lane == 0) {
-    cursor[0] = nq;
+    cursor[0] = nq;  // level 1 lists every candidate in order; P starts at nq
+    aoff[0] = 0;
+    alen[0] = nsub;
+    atop[0] = nsub;
+    rsum[0] = sR0;
+    rcnt[0] = (uint32_t)nR0;
   }
   if (lane < K) {
     int bits = n - 32 * lane;
@@ -120,19 +141,27 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
     uint32_t Lm[K];
 #pragma unroll
     for (int w = 0; w < K; ++w) Lm[w] = lmask[(level - 1) * K + w];
-    int cur = -1;
-    for (int b0 = cursor[level - 1]; b0 < nsub; b0 += 32) {
-      int i = b0 + lane;
+    const int* A = act + aoff[level - 1];
+    const int na = alen[level - 1];
+    int cur = -1, curpos = -1;
+    for (int b0 = cursor[level - 1]; b0 < na; b0 += 32) {
+      int q = b0 + lane;
       bool ok = false;
-      if (i < nsub && bound[i] > level - 1) {
-        uint32_t any = 0;
+      int i = 0;
+      if (q < na) {
+        i = A[q];
+        if (bound[i] > level - 1) {
+          uint32_t any = 0;
 #pragma unroll
-        for (int w = 0; w < K; ++w) any |= masks[(size_t)w * capC + i] & Lm[w];
-        ok = any != 0;
+          for (int w = 0; w < K; ++w) any |= masks[(size_t)w * capC + i] & Lm[w];
+          ok = any != 0;
+        }
       }
       unsigned bal = __ballot_sync(kFull, ok);
       if (bal) {
-        cur = b0 + __ffs(bal) - 1;
+        int src = __ffs(bal) - 1;
+        curpos = b0 + src;
+        cur = __shfl_sync(kFull, i, src);
         break;
       }
     }
@@ -145,24 +174,44 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
         Ln[w] = Lm[w] & masks[(size_t)w * capC + cur];
         kn += __popc(Ln[w]);
       }
+      // Child list goes above everything the stack holds.
+      const int ctop = atop[level - 1];
+      const bool fits = ctop + na <= actcap;
       bool ism = true;
       uint64_t sR = 0;
       unsigned long long nR = 0;
-      for (int i = lane; i < nsub; i += 32) {
-        bool cover = true;
+      int nchild = 0, nbefore = 0;  // child list size; entries before cur in it
+      for (int b0 = 0; b0 < na; b0 += 32) {
+        int q = b0 + lane;
+        bool keep = false;
+        int i = 0;
+        if (q < na) {
+          i = A[q];
+          bool cover = true, meet = false;
 #pragma unroll
-        for (int w = 0; w < K; ++w) cover &= (masks[(size_t)w * capC + i] & Ln[w]) == Ln[w];
-        if (cover) {
-          sR += subkey[i];
-          ++nR;
+          for (int w = 0; w < K; ++w) {
+            uint32_t m = masks[(size_t)w * capC + i] & Ln[w];
+            cover &= m == Ln[w];
+            meet |= m != 0;
+          }
           int b = bound[i];
-          if (i < cur && b >= level) ism = false;
-          else if (b > level) bound[i] = level;
+          if (cover) {
+            sR += subkey[i];
+            ++nR;
+            if (i < cur && b >= level) ism = false;
+            else if (b > level) bound[i] = level;
+          } else {
+            keep = meet && b > level;
+          }
         }
+        unsigned bal = __ballot_sync(kFull, keep);
+        if (fits && keep) act[ctop + nchild + __popc(bal & lanemask_lt())] = i;
+        nchild += __popc(bal);
+        nbefore += __popc(__ballot_sync(kFull, keep && i < cur));
       }
       ism = __all_sync(kFull, ism);
-      sR = warp_sum(sR) + sR0;
-      nR = warp_sum(nR) + nR0;
+      sR = warp_sum(sR) + rsum[level - 1];
+      nR = warp_sum(nR) + rcnt[level - 1];
       if (ism) {
         uint64_t sL = 0;
 #pragma unroll
@@ -175,10 +224,23 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
         W.nonmax += 1;
       }
       __syncwarp();
-      if (ism && kn > 1) {
+      if (ism && kn > 1 && nchild > 0) {
         if (lane == 0) {
-          cursor[level - 1] = cur;
-          cursor[level] = cur + 1;
+          cursor[level - 1] = curpos;
+          // The child level takes candidates after cur (exe_stack[level] =
+          // cur + 1); lists are in index order, so skip the entries before it.
+          cursor[level] = fits ? nbefore : curpos + 1;
+          rsum[level] = sR;
+          rcnt[level] = (uint32_t)nR;
+          if (fits) {
+            aoff[level] = ctop;
+            alen[level] = nchild;
+            atop[level] = ctop + nchild;
+          } else {
+            aoff[level] = aoff[level - 1];
+            alen[level] = na;
+            atop[level] = ctop;
+          }
         }
         if (lane < K) {
           uint32_t v = 0;
@@ -191,34 +253,34 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
         ++level;
         continue;
       }
-      if (lane == 0) cursor[level - 1] = cur + 1;
+      if (lane == 0) cursor[level - 1] = curpos + 1;
     } else {
       --level;
       if (level == 0) break;
-      cur = cursor[level - 1];
+      int cp = cursor[level - 1];
+      cur = act[aoff[level - 1] + cp];
       __syncwarp();
-      if (lane == 0) cursor[level - 1] = cur + 1;
+      if (lane == 0) cursor[level - 1] = cp + 1;
     }
     // ---- pop (finder_pop) of candidate `cur` at `level` ----
-    uint32_t rem[K];
-    bool rem_any = false;
+    {
+      const int* A = act + aoff[level - 1];
+      const int na = alen[level - 1];
+      uint32_t rem[K];
 #pragma unroll
-    for (int w = 0; w < K; ++w) {
-      uint32_t lp = lmask[(level - 1) * K + w];
-      rem[w] = lp & ~masks[(size_t)w * capC + cur];
-      rem_any |= rem[w] != 0;
-    }
-    (void)rem_any;
-    for (int i = lane; i < nsub; i += 32) {
-      int b = bound[i];
-      if (b >= level) {
-        if (prune) {
-          uint32_t t = 0;
+      for (int w = 0; w < K; ++w) rem[w] = lmask[(level - 1) * K + w] & ~masks[(size_t)w * capC + cur];
+      for (int q = lane; q < na; q += 32) {
+        int i = A[q];
+        int b = bound[i];
+        if (b >= level) {
+          if (prune) {
+            uint32_t t = 0;
 #pragma unroll
-          for (int w = 0; w < K; ++w) t |= masks[(size_t)w * capC + i] & rem[w];
-          bound[i] = (t != 0 || i == cur) ? kFree : level - 1;
-        } else {
-          bound[i] = kFree;
+            for (int w = 0; w < K; ++w) t |= masks[(size_t)w * capC + i] & rem[w];
+            bound[i] = (t != 0 || i == cur) ? kFree : level - 1;
+          } else {
+            bound[i] = kFree;
+          }
         }
       }
     }
@@ -391,6 +453,151 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
   __syncwarp();
 }
 
+// A push at `level` whose child L (the `kept` rows, marked llevel == level)
+// fits the bitmap tier, done without touching the level's counts: the child's
+// neighbour counts are built from the kept rows alone, the child sub-problem
+// goes to tier 2, and the state after finder_pop is written directly.  With
+// pruning on, finder_pop leaves a candidate c of bound >= level at FREE if c
+// is adjacent to a removed vertex (its count inside the kept rows is below
+// its count at this level) or is x itself, and at level-1 otherwise; every
+// candidate of bound >= level is FREE before the push, and candidates not
+// adjacent to the kept rows are either touched (stay FREE) or irrelevant
+// below this level (count 0), so only candidates adjacent to the kept rows
+// change.
+__device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept, uint64_t sL) {
+  const int lane = (int)lane_id();
+  int32_t* llevel = W.A(W.sl.llevel);
+  const int32_t* ncnt = W.A(W.sl.ncnt);
+  int32_t* bound = W.A(W.sl.bound);
+  const int32_t* cv = W.A(W.sl.cv);
+  const int32_t* coff = W.A(W.sl.coff);
+  const int32_t* cadj = W.A(W.sl.cadj);
+  const int32_t* aoff = W.A(W.sl.aoff);
+  const int32_t* aadj = W.A(W.sl.aadj);
+  int32_t* cc = W.A(W.sl.fill);   // child counts, all-zero between pushes
+  int32_t* sidx = W.A(W.sl.sidx); // -1 between pushes
+  int32_t* tl = W.A(W.sl.tlist);
+  int32_t* lp = W.A(W.sl.lp);
+  uint64_t* lkey = W.A64(W.sl.lkey);
+  uint64_t* subkey = W.A64(W.sl.sub_v);
+  // kept rows -> lp[0..kept), with their hash keys
+  int n = 0;
+  {
+    int rb = coff[x], re = coff[x + 1];
+    for (int b0 = rb; b0 < re; b0 += 32) {
+      int j = b0 + lane;
+      int l = j < re ? cadj[j] : 0;
+      bool sel = j < re && llevel[l] == level;
+      unsigned bal = __ballot_sync(kFull, sel);
+      if (sel) {
+        int q = n + __popc(bal & lanemask_lt());
+        lp[q] = l;
+        if (q < 32 * kKMax) lkey[q] = W.g.ukey[t.L[l]];
+      }
+      n += __popc(bal);
+    }
+  }
+  __syncwarp();
+  // child counts over the kept rows; tl = candidates met
+  int nt = 0;
+  flat_rows(
+      n,
+      [&](int r, int& beg, int& len) {
+        int l = lp[r];
+        beg = aoff[l];
+        len = aoff[l + 1] - beg;
+      },
+      [&](bool valid, int, int pos) {
+        int p = valid ? aadj[pos] : -1;
+        bool first = false;
+        if (p >= 0) first = atomicAdd(&cc[p], 1) == 0;
+        unsigned bal = __ballot_sync(kFull, first);
+        if (first) tl[nt + __popc(bal & lanemask_lt())] = p;
+        nt += __popc(bal);
+      });
+  __syncwarp();
+  // R of the child, maximality, and the child's candidates (Q part first)
+  bool ism = true;
+  uint64_t sR = 0;
+  unsigned long long nR = 0;
+  int nq = 0, np = 0, ncand = 0;
+  for (int b0 = 0; b0 < nt; b0 += 32) {
+    int q = b0 + lane;
+    bool isC = false;
+    if (q < nt) {
+      int p = tl[q];
+      int c = cc[p];
+      if (c == kept) {
+        sR += W.g.vkey[cv[p]];
+        ++nR;
+        if (p < x && bound[p] >= level) ism = false;
+      } else {
+        isC = bound[p] >= level;
+      }
+    }
+    ncand += __popc(__ballot_sync(kFull, isC));
+  }
+  ism = __all_sync(kFull, ism);
+  sR = warp_sum(sR) + t.sRtask;
+  nR = warp_sum(nR) + t.nRtask;
+  if (ism) {
+    W.cnt += 1;
+    W.hash += biclique_hash(W.g, sL, (uint64_t)kept, sR, nR);
+  } else {
+    W.nonmax += 1;
+  }
+  if (ism && kept > 1 && ncand > 0) {
+    for (int b0 = 0; b0 < nt; b0 += 32) {
+      int q = b0 + lane;
+      int p = q < nt ? tl[q] : 0;
+      bool isC = q < nt && cc[p] != kept && bound[p] >= level;
+      bool isQ = isC && p < x;
+      bool isP = isC && p > x;
+      unsigned bq = __ballot_sync(kFull, isQ);
+      unsigned bp = __ballot_sync(kFull, isP);
+      int s = -1;
+      if (isQ) s = nq + __popc(bq & lanemask_lt());
+      if (isP) s = ncand - 1 - (np + __popc(bp & lanemask_lt()));
+      if (s >= 0) {
+        sidx[p] = s;
+        subkey[s] = W.g.vkey[cv[p]];
+      }
+      nq += __popc(bq);
+      np += __popc(bp);
+    }
+    __syncwarp();
+    clear_masks(W, n, ncand);
+    uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+    const int capC = W.sl.capC;
+    flat_rows(
+        n,
+        [&](int r, int& beg, int& len) {
+          int l = lp[r];
+          beg = aoff[l];
+          len = aoff[l + 1] - beg;
+        },
+        [&](bool valid, int r, int pos) {
+          if (!valid) return;
+          int p = aadj[pos];
+          if (p < 0) return;
+          int si = sidx[p];
+          if (si >= 0) atomicOr(&masks[(size_t)(r >> 5) * capC + si], 1u << (r & 31));
+        });
+    __syncwarp();
+    tier2(W, n, ncand, nq, sR, nR);
+  }
+  __syncwarp();
+  // state after finder_pop(x, level), then clear the child scratch
+  for (int q = lane; q < nt; q += 32) {
+    int p = tl[q];
+    if (bound[p] >= level && p != x && cc[p] == ncnt[p]) bound[p] = level - 1;
+    cc[p] = 0;
+    sidx[p] = -1;
+  }
+  for (int q = lane; q < n; q += 32) llevel[lp[q]] = level - 1;
+  __syncwarp();
+}
+
 __device__ void tier1_run(Warp& W, const T1& t) {
   const int lane = (int)lane_id();
   int32_t* llevel = W.A(W.sl.llevel);
@@ -439,6 +646,12 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       kept = warp_sum(kept);
       sL = warp_sum(sL);
       __syncwarp();
+      if (W.p.prune && kept <= t2max) {
+        t1_sparse_push(W, t, cur, level, kept, sL);
+        if (lane == 0) stack[level - 1] = cur + 1;
+        __syncwarp();
+        continue;
+      }
       int nLp = lsize[level - 1];
       bool recompute = nLp > 2 * kept;
       if (recompute) {
@@ -924,6 +1137,9 @@ __device__ void run_task(Warp& W, const Task& t) {
             cadj[coff[p] + s] = r;
           });
       __syncwarp();
+      // fill doubles as the sparse push's child-count array: back to zero.
+      for (int i = lane; i < nC; i += 32) fill[i] = 0;
+      __syncwarp();
       T1 t1;
       t1.L = L;
       t1.nL = nL;
@@ -959,6 +1175,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   W.cnt = W.hash = W.nonmax = W.splits = 0;
   const int nroots = g.n_roots;
   uint64_t idle_since = 0;
+  uint64_t busy_ns = 0, last_done_ns = 0;
   while (true) {
     int ab = lane == 0 ? *(volatile int32_t*)&ctl->abort : 0;
     if (__shfl_sync(kFull, ab, 0)) break;
@@ -982,8 +1199,12 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     if (have) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) t.v[i] = __shfl_sync(kFull, t.v[i], 0);
+      uint64_t tb = globaltimer_ns();
       run_task(W, t);
       __syncwarp();
+      uint64_t te = globaltimer_ns();
+      busy_ns += te - tb;
+      last_done_ns = te - t_start;
       if (lane == 0) {
         __threadfence();
         atomicAdd(&ctl->pending, (unsigned long long)-1LL);
@@ -1017,8 +1238,22 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     if (W.splits) atomicAdd(&ctl->tasks_split, W.splits);
   }
   if (p.record_exit) {
+    // Per block: when its last task finished, and its warps' summed busy time.
+    __shared__ unsigned long long blk_last, blk_busy;
+    if (threadIdx.x == 0) {
+      blk_last = 0;
+      blk_busy = 0;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) exit_ns[blockIdx.x] = globaltimer_ns() - t_start;
+    if (lane == 0) {
+      atomicMax(&blk_last, (unsigned long long)last_done_ns);
+      atomicAdd(&blk_busy, (unsigned long long)busy_ns);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      exit_ns[blockIdx.x] = blk_last;
+      exit_ns[gridDim.x + blockIdx.x] = blk_busy;
+    }
   }
 }
 

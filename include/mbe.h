@@ -98,8 +98,9 @@ typedef struct mbe_result {
   double enum_seconds;   /* host wall time of mbe_enumerate (reference: exe_time_) */
   float kernel_ms;       /* CUDA-event time of the enumeration kernel(s) */
   int32_t status;        /* device status word (0 = OK) */
-  double sm_exit_max_ms; /* -p: slowest block's exit time, ms after launch */
-  double sm_exit_min_ms; /* -p: fastest block's exit time */
+  double sm_exit_max_ms; /* -p: latest time a block finished its last task, ms after launch */
+  double sm_exit_min_ms; /* -p: earliest such time (max - min = load-balance skew) */
+  double warp_busy_frac; /* -p: share of warp-time spent inside tasks */
 } mbe_result;
 
 /* Default parameters: bound_height 20, bound_size 1500, prune 1. */
