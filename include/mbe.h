@@ -139,6 +139,43 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out);
 /* Thread-local message of the last failed call ("" if none). */
 const char* mbe_last_error_string(void);
 
+/* Enumeration that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code inside a framework whose own
+ * allocator owns all device memory, code that is recorded into a CUDA graph,
+ * or a process whose device-memory budget is fixed up front.  mbe_enumerate
+ * allocates (and caches) its workspace; this call instead takes every working
+ * buffer from one static device pool of 64 MiB built into the library, which
+ * every GPU that loads the library holds until the process exits.
+ *
+ * Inputs (device memory, owned by the caller), in the engine's numbering with
+ * no side swap or reordering, roots = V rows:
+ *   d_row_off[nV+1], d_col[nE]   V -> U rows, strictly ascending U ids
+ *   d_rev_off[nU+1], d_rev_col[nE] its transpose (U -> V rows, ascending)
+ *   max_two_hop   optional bound on sum_{u in N(v)} d(u) over all roots v
+ *                 (0 = use nE); a tighter bound lets more warps fit the pool
+ *   params        NULL = defaults; sm_timing, queue_capacity, root range and
+ *                 shards are ignored (all roots, fixed 4096-entry split ring)
+ * Output (device memory, owned by the caller): d_out[4] = count, set hash,
+ * non-maximal branches, device status (0 = OK, else a device error code).
+ * Ids in the hash are the input ids.
+ *
+ * The work is queued on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and the call returns without waiting: read d_out after the stream
+ * completes.  The call fails with MBE_ERR_CAPACITY, before queuing anything,
+ * when one 16-warp block's scratch for this graph (roughly
+ * 4*(20*nV + 2*max_two_hop) bytes per warp) plus the hash keys do not fit
+ * the pool.  The first call on each device looks up the pool's device
+ * address with that device current; make that first call before any stream
+ * capture.  Every call on a device shares the one pool, which keeps the last
+ * call's contents (each call clears what must start at zero): calls whose
+ * work overlaps on the GPU race on it and must be serialised by the caller
+ * (one stream, or events). */
+int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int32_t* d_col, int32_t nV,
+                                 const int32_t* d_rev_off, const int32_t* d_rev_col, int32_t nU,
+                                 int64_t nE, int64_t max_two_hop, const mbe_params* params,
+                                 unsigned long long* d_out, void* stream);
+
 /* ---- synthetic inputs ------------------------------------------------------
  * Seeded Chung-Lu bipartite generator (splitmix64 stream, Vose alias
  * sampling): expected degree of vertex i proportional to (i+1)^(-1/(gamma-1)),
