@@ -166,6 +166,23 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case():
+    """A reduced launch of the same kernel for ncu captures: 16 blocks and a
+    stratified 1/64 share of the medium graph's roots, one warm-up and one
+    profiled enumeration.  Sized so ncu's multi-pass replay stays within a
+    few GB of device memory and a minute or two."""
+    import gmbe_b200 as gm
+    g = gm.config_graph(WORKLOAD)
+    with gm.Graph.from_csr(g.row_off, g.col, g.nU, **FLAGS) as G:
+        kw = dict(blocks=16, shard_count=64, shard_index=0)
+        a = G.enumerate(**kw)
+        b = G.enumerate(**kw)
+    if (a.count, a.set_hash) != (b.count, b.set_hash):
+        raise SystemExit("profile case not reproducible")
+    print(json.dumps({"profile_case": "medium, 16 blocks, roots p = 0 mod 64", "count": b.count,
+                      "set_hash": f"{b.set_hash:#x}", "kernel_ms": b.kernel_ms}), flush=True)
+
+
 def WORKLOAD_DESC():
     import gmbe_b200 as gm
     return gm.DESCRIPTIONS[WORKLOAD]
@@ -178,9 +195,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="one reduced launch for ncu: 16 blocks, every 64th root (~1.6 GB scratch)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.profile:
+        run_profile_case()
         return
 
     import numpy as np

@@ -56,7 +56,8 @@ class Params(C.Structure):
                 ("blocks", C.c_int32), ("queue_capacity", C.c_int32),
                 ("bitmap_max_l", C.c_int32), ("wait_limit_ns", C.c_int64),
                 ("sm_timing", C.c_int32), ("root_begin", C.c_int32), ("root_end", C.c_int32),
-                ("shard_count", C.c_int32), ("shard_index", C.c_int32)]
+                ("shard_count", C.c_int32), ("shard_index", C.c_int32),
+                ("split_mode", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -64,7 +65,11 @@ class Result(C.Structure):
                 ("tasks_split", C.c_uint64), ("enum_seconds", C.c_double),
                 ("kernel_ms", C.c_float), ("status", C.c_int32),
                 ("sm_exit_max_ms", C.c_double), ("sm_exit_min_ms", C.c_double),
-                ("warp_busy_frac", C.c_double)]
+                ("warp_busy_frac", C.c_double), ("setup_ms", C.c_double),
+                ("tier1_ms", C.c_double), ("tier2_ms", C.c_double), ("idle_ms", C.c_double),
+                ("max_task_ms", C.c_double), ("max_task_root", C.c_int32),
+                ("max_task_degree", C.c_int32), ("n_tasks", C.c_uint64),
+                ("n_subproblems", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

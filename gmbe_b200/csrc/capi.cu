@@ -79,6 +79,9 @@ struct Workspace {
   unsigned long long* exit_ns = nullptr;
   int32_t exit_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int32_t* slots = nullptr;  // exported bitmap sub-problems
+  uint32_t* slot_bits = nullptr;
+  int32_t nslot = 0;
   // Layout the per-warp count maps were last cleared for.
   int64_t map_pitch_words = -1, map_words = -1;
   int32_t map_warps = -1;
@@ -343,6 +346,13 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
     ws.q_cap = qcap;
   }
   if (!ws.ctl) CK(cudaMalloc((void**)&ws.ctl, sizeof(EnumCtl)));
+  if (!ws.slots) {
+    const int32_t nslot = 4096;  // 4096 x 64 KiB = 256 MiB
+    CK(cudaMalloc((void**)&ws.slots, sizeof(int32_t) * (size_t)kSlotWordsHost * nslot));
+    CK(cudaMalloc((void**)&ws.slot_bits, sizeof(uint32_t) * (size_t)(nslot / 32)));
+    ws.nslot = nslot;
+  }
+  CK(cudaMemsetAsync(ws.slot_bits, 0, sizeof(uint32_t) * (size_t)(ws.nslot / 32)));
   if (blocks > ws.exit_cap) {
     cudaFree(ws.exit_ns);
     ws.exit_ns = nullptr;
@@ -380,8 +390,13 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   ep.tier2_max_l = t2;
 
   CK(cudaEventRecord(ws.ev0));
-  mbe_enum_kernel<<<blocks, kEnumThreads>>>(dg, ep, sl, ws.ctl, ws.q_tasks, ws.q_seq, ws.scratch,
-                                            ws.exit_ns);
+  SlotPool pool;
+  pool.slots = ws.slots;
+  pool.bits = ws.slot_bits;
+  pool.nslot = prm.split_mode == 1 ? 0 : ws.nslot;
+  ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
+  mbe_enum_kernel<<<blocks, kEnumThreads>>>(dg, ep, sl, ws.ctl, ws.q_tasks, ws.q_seq, pool,
+                                            ws.scratch, ws.exit_ns);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ws.ev1));
   EnumCtl ctl;
@@ -394,6 +409,15 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   out->tasks_split = ctl.tasks_split;
   out->kernel_ms = ms;
   out->status = ctl.status;
+  out->setup_ms = ctl.ns_setup / 1e6;
+  out->tier1_ms = ctl.ns_tier1 / 1e6;
+  out->tier2_ms = ctl.ns_tier2 / 1e6;
+  out->idle_ms = ctl.ns_idle / 1e6;
+  out->max_task_ms = ctl.max_task_ns / 1e6;
+  out->max_task_root = (int32_t)(ctl.max_task_info >> 32);
+  out->max_task_degree = (int32_t)(ctl.max_task_info & 0xffffffffu);
+  out->n_tasks = ctl.n_tasks;
+  out->n_subproblems = ctl.n_tier2;
   if (prm.sm_timing) {
     std::vector<unsigned long long> ex(2 * (size_t)blocks);
     CK(cudaMemcpy(ex.data(), ws.exit_ns, 2 * sizeof(unsigned long long) * blocks,

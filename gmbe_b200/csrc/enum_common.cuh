@@ -46,12 +46,17 @@ struct EnumCtl {
   int32_t next_root;     // roots handed out so far (descending internal id)
   int32_t status;        // first error code
   int32_t abort;         // set together with status
-  int32_t pad0;
+  int32_t idle_warps;    // warps waiting for work (export demand)
   unsigned long long pending;   // queued + running tasks (termination)
   unsigned long long q_head;    // next slot to consume
   unsigned long long q_tail;    // next slot to produce
   unsigned long long q_used;    // reserved and not yet consumed slots
   unsigned long long err_info;  // diagnostic of the first error
+  // profile counters (summed warp-time in ns, longest task)
+  unsigned long long ns_setup, ns_tier1, ns_tier2, ns_idle;
+  unsigned long long max_task_ns;   // longest single task
+  unsigned long long max_task_info; // (root << 32) | |L| of that task
+  unsigned long long n_tasks, n_tier2;
 };
 
 // Per-warp scratch layout (int32 words unless noted), offsets in words from
@@ -69,6 +74,13 @@ struct ScratchLayout {
   int32_t act_cap, pad;
 };
 
+// Slots for bitmap sub-problems handed to idle warps.
+struct SlotPool {
+  int32_t* slots;  // nslot x 16384 int32 words
+  uint32_t* bits;  // occupancy, nslot / 32 words, zero at launch
+  int32_t nslot;   // multiple of 32; 0 disables export
+};
+
 struct EnumParams {
   int32_t bound_height, bound_size, prune;
   int32_t queue_cap;
@@ -76,6 +88,8 @@ struct EnumParams {
   int64_t idle_ns_limit;      // nanoseconds a warp may idle waiting for work
   int32_t record_exit;        // -p
   int32_t tier2_max_l;        // |L| at or below which the bitmap tier runs (<= 32*kmax)
+  int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
+  int32_t pad;
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

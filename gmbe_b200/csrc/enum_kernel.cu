@@ -80,13 +80,154 @@ struct Warp {
   EnumCtl* ctl;
   Task* q_tasks;
   unsigned long long* q_seq;
+  int32_t* slots;        // exported bitmap sub-problems (nslot x slot_words)
+  uint32_t* slot_bits;   // slot occupancy
+  int nslot;
   int32_t* base;
   // accumulators (uniform over lanes)
   unsigned long long cnt, hash, nonmax, splits;
+  unsigned long long ns_t2, n_t2;  // time inside the bitmap tier, sub-problems run
+  unsigned long long ns_t1;        // time inside the counts tier (bitmap tier excluded)
 
   __device__ int32_t* A(int64_t off) const { return base + off; }
   __device__ uint64_t* A64(int64_t off) const { return reinterpret_cast<uint64_t*>(base + off); }
 };
+
+// ---------------------------------------------------------------------------
+// Bitmap sub-problems and their export to idle warps.
+struct T2Src {
+  const uint32_t* masks;  // masks[w * stride + i]: word w of candidate i inside L
+  int stride;
+  const uint64_t* subkey;  // hash key of candidate i
+  const uint64_t* lkey;    // hash key of L bit b
+  uint32_t L0[4];          // the sub-problem's L
+  int nsub, nq;            // candidates [0, nq) are Q, [nq, nsub) P
+  uint64_t sR0;            // R of the sub-problem's root biclique
+  uint32_t nR0;
+};
+
+// Slot layout (int32 words): header, lkey (128 x uint64), masks (K x stride), subkey.
+constexpr int kSlotWords = 16384;
+constexpr int kSlotHdr = 16;
+constexpr int kSlotLkey = kSlotHdr;
+constexpr int kSlotMasks = kSlotLkey + 2 * 32 * 4;
+__host__ __device__ constexpr int slot_stride_max(int K) {
+  return ((kSlotWords - kSlotMasks) / (K + 2)) & ~31;
+}
+// header words: 0 K, 1 nsub, 2 nq, 3 stride, 4..7 L0, 8..9 sR0, 10 nR0
+
+// Claims a free slot (lane 0); -1 if none.
+__device__ int slot_alloc(Warp& W) {
+  const int nw = W.nslot >> 5;
+  if (nw == 0) return -1;
+  int start = (int)(((blockIdx.x * 32u + (threadIdx.x >> 5)) * 2654435761u) % (unsigned)nw);
+  for (int t = 0; t < nw; ++t) {
+    int wi = (start + t) % nw;
+    unsigned cur = *(volatile unsigned*)&W.slot_bits[wi];
+    while (cur != 0xffffffffu) {
+      int b = __ffs(~cur) - 1;
+      unsigned old = atomicOr(&W.slot_bits[wi], 1u << b);
+      if (!(old & (1u << b))) return wi * 32 + b;
+      cur = old | (1u << b);
+    }
+  }
+  return -1;
+}
+
+__device__ void slot_free(Warp& W, int s) { atomicAnd(&W.slot_bits[s >> 5], ~(1u << (s & 31))); }
+
+__device__ bool queue_push_one(Warp& W, const Task& t);
+
+// True when idle warps outnumber queued work (lane-uniform).
+__device__ bool export_wanted(Warp& W) {
+  int want = 0;
+  if (lane_id() == 0) {
+    EnumCtl* c = W.ctl;
+    int idle = *(volatile int32_t*)&c->idle_warps;
+    unsigned long long queued = *(volatile unsigned long long*)&c->q_tail -
+                                *(volatile unsigned long long*)&c->q_head;
+    want = idle > 0 && (unsigned long long)idle > queued;
+  }
+  return __shfl_sync(0xffffffffu, want, 0) != 0;
+}
+
+// GMBE's split test on a child: (|P| > h or |L| > h) and |P| * |L| > s.
+__device__ __forceinline__ bool big_enough(const Warp& W, int nP, int nL) {
+  return (nP > W.p.bound_height || nL > W.p.bound_height) &&
+         (long long)nP * nL > (long long)W.p.bound_size;
+}
+
+// Writes a slot header and enqueues it; frees the slot if the ring is full.
+__device__ bool slot_publish(Warp& W, int slot) {
+  __syncwarp();
+  __threadfence();
+  Task t;
+  t.v[0] = -2 - slot;
+  t.v[1] = t.v[2] = t.v[3] = -1;
+  return queue_push_one(W, t);
+}
+
+// Exports the child (list of candidate indices `child`, Ln, base R) of a
+// first-level push of a bitmap sub-problem.  The child's candidates keep
+// their order, so its first nbefore entries are its Q part.
+template <int K>
+__device__ bool t2_try_export(Warp& W, const T2Src& src, const int* child, int nchild, int nbefore,
+                              const uint32_t* Ln, int kn, uint64_t sR, uint64_t nR) {
+  if (nchild > slot_stride_max(K) || !big_enough(W, nchild - nbefore, kn) || !export_wanted(W))
+    return false;
+  const int lane = (int)lane_id();
+  int slot = lane == 0 ? slot_alloc(W) : 0;
+  slot = __shfl_sync(0xffffffffu, slot, 0);
+  if (slot < 0) return false;
+  int32_t* sp = W.slots + (size_t)slot * kSlotWords;
+  const int stride = (nchild + 31) & ~31;
+  uint32_t* m = reinterpret_cast<uint32_t*>(sp + kSlotMasks);
+  uint64_t* key = reinterpret_cast<uint64_t*>(sp + kSlotMasks + K * stride);
+  uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
+  for (int q = lane; q < nchild; q += 32) {
+    int i = child[q];
+#pragma unroll
+    for (int w = 0; w < K; ++w) m[(size_t)w * stride + q] = src.masks[(size_t)w * src.stride + i];
+    key[q] = src.subkey[i];
+  }
+  for (int b = lane; b < 32 * K; b += 32) lk[b] = src.lkey[b];
+  if (lane == 0) {
+    sp[0] = K;
+    sp[1] = nchild;
+    sp[2] = nbefore;
+    sp[3] = stride;
+    for (int w = 0; w < 4; ++w) sp[4 + w] = w < K ? (int32_t)Ln[w] : 0;
+    *reinterpret_cast<uint64_t*>(sp + 8) = sR;
+    sp[10] = (int32_t)nR;
+  }
+  (void)kn;
+  if (slot_publish(W, slot)) return true;
+  if (lane == 0) slot_free(W, slot);
+  __syncwarp();
+  return false;
+}
+
+__device__ void tier2_dispatch(Warp& W, const T2Src& src, int words);
+
+// Runs an exported sub-problem and releases its slot.
+__device__ void tier2_from_slot(Warp& W, int slot) {
+  const int32_t* sp = W.slots + (size_t)slot * kSlotWords;
+  T2Src src;
+  const int K = sp[0];
+  src.nsub = sp[1];
+  src.nq = sp[2];
+  src.stride = sp[3];
+  for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)sp[4 + w];
+  src.sR0 = *reinterpret_cast<const uint64_t*>(sp + 8);
+  src.nR0 = (uint32_t)sp[10];
+  src.lkey = reinterpret_cast<const uint64_t*>(sp + kSlotLkey);
+  src.masks = reinterpret_cast<const uint32_t*>(sp + kSlotMasks);
+  src.subkey = reinterpret_cast<const uint64_t*>(sp + kSlotMasks + K * src.stride);
+  tier2_dispatch(W, src, K);
+  __syncwarp();
+  if (lane_id() == 0) slot_free(W, slot);
+  __syncwarp();
+}
 
 // ---------------------------------------------------------------------------
 // Tier 2: bitmap DFS over a sub-problem with n <= 32*K vertices in L.
@@ -99,13 +240,14 @@ struct Warp {
 // only what can still matter.  A level whose list does not fit the arena
 // shares its parent's list (a superset; the scans re-test the mask).
 template <int K>
-__device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
+__device__ void tier2_run(Warp& W, const T2Src& src) {
   const int lane = (int)lane_id();
-  const int capC = W.sl.capC;
-  const uint32_t* masks = reinterpret_cast<const uint32_t*>(W.A(W.sl.masks));
-  const uint64_t* subkey = W.A64(W.sl.sub_v);
+  const int capC = src.stride;
+  const uint32_t* masks = src.masks;
+  const uint64_t* subkey = src.subkey;
   int32_t* bound = W.A(W.sl.bound2);
-  const uint64_t* lkey = W.A64(W.sl.lkey);
+  const uint64_t* lkey = src.lkey;
+  const int nsub = src.nsub, nq = src.nq;
   uint32_t* lmask = reinterpret_cast<uint32_t*>(W.A(W.sl.lmask));
   int32_t* cursor = W.A(W.sl.cursor2);   // position inside the level's active list
   int32_t* aoff = W.A(W.sl.act_off);     // level list start in the arena
@@ -128,12 +270,15 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
     aoff[0] = 0;
     alen[0] = nsub;
     atop[0] = nsub;
-    rsum[0] = sR0;
-    rcnt[0] = (uint32_t)nR0;
+    rsum[0] = src.sR0;
+    rcnt[0] = src.nR0;
   }
   if (lane < K) {
-    int bits = n - 32 * lane;
-    lmask[lane] = bits >= 32 ? 0xffffffffu : (bits <= 0 ? 0u : ((1u << bits) - 1u));
+    uint32_t v = 0;
+#pragma unroll
+    for (int w = 0; w < K; ++w)
+      if (w == lane) v = src.L0[w];
+    lmask[lane] = v;
   }
   __syncwarp();
   int level = 1;
@@ -224,7 +369,12 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
         W.nonmax += 1;
       }
       __syncwarp();
-      if (ism && kn > 1 && nchild > 0) {
+      // A big enough child of the sub-problem's first level goes to an idle
+      // warp instead (the state after the pop below does not depend on it).
+      bool exported = false;
+      if (ism && kn > 1 && nchild > 0 && fits && level == 1)
+        exported = t2_try_export<K>(W, src, act + ctop, nchild, nbefore, Ln, kn, sR, nR);
+      if (ism && kn > 1 && nchild > 0 && !exported) {
         if (lane == 0) {
           cursor[level - 1] = curpos;
           // The child level takes candidates after cur (exe_stack[level] =
@@ -288,15 +438,32 @@ __device__ void tier2_run(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64
   }
 }
 
-template <int K>
-__device__ void tier2_dispatch_k(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
-  tier2_run<K>(W, n, nsub, nq, sR0, nR0);
+__device__ void tier2_dispatch(Warp& W, const T2Src& src, int words) {
+  uint64_t t0 = globaltimer_ns();
+  if (words <= 1) tier2_run<1>(W, src);
+  else if (words <= 2) tier2_run<2>(W, src);
+  else tier2_run<4>(W, src);
+  W.ns_t2 += globaltimer_ns() - t0;
+  W.n_t2 += 1;
 }
 
+// Sub-problem built in the warp's own scratch over n L vertices (all bits set).
 __device__ void tier2(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
-  if (n <= 32) tier2_dispatch_k<1>(W, n, nsub, nq, sR0, nR0);
-  else if (n <= 64) tier2_dispatch_k<2>(W, n, nsub, nq, sR0, nR0);
-  else tier2_dispatch_k<4>(W, n, nsub, nq, sR0, nR0);
+  T2Src src;
+  src.masks = reinterpret_cast<const uint32_t*>(W.A(W.sl.masks));
+  src.stride = W.sl.capC;
+  src.subkey = W.A64(W.sl.sub_v);
+  src.lkey = W.A64(W.sl.lkey);
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    int bits = n - 32 * w;
+    src.L0[w] = bits >= 32 ? 0xffffffffu : (bits <= 0 ? 0u : ((1u << bits) - 1u));
+  }
+  src.nsub = nsub;
+  src.nq = nq;
+  src.sR0 = sR0;
+  src.nR0 = (uint32_t)nR0;
+  tier2_dispatch(W, src, (n + 31) >> 5);
 }
 
 // Zeroes the masks of candidates [0, nsub) for n vertices.
@@ -520,12 +687,13 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   bool ism = true;
   uint64_t sR = 0;
   unsigned long long nR = 0;
-  int nq = 0, np = 0, ncand = 0;
+  int nq = 0, np = 0, ncand = 0, nqc = 0;
   for (int b0 = 0; b0 < nt; b0 += 32) {
     int q = b0 + lane;
     bool isC = false;
+    int p = 0;
     if (q < nt) {
-      int p = tl[q];
+      p = tl[q];
       int c = cc[p];
       if (c == kept) {
         sR += W.g.vkey[cv[p]];
@@ -536,6 +704,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       }
     }
     ncand += __popc(__ballot_sync(kFull, isC));
+    nqc += __popc(__ballot_sync(kFull, isC && p < x));
   }
   ism = __all_sync(kFull, ism);
   sR = warp_sum(sR) + t.sRtask;
@@ -547,6 +716,26 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
     W.nonmax += 1;
   }
   if (ism && kept > 1 && ncand > 0) {
+    // Destination: an export slot when idle warps want work and the child is
+    // big enough by GMBE's split test, else this warp's scratch.
+    const int words = (n + 31) >> 5;
+    const int K = words <= 1 ? 1 : (words <= 2 ? 2 : 4);
+    int slot = -1;
+    if (ncand <= slot_stride_max(K) && big_enough(W, ncand - nqc, n) && export_wanted(W)) {
+      slot = lane == 0 ? slot_alloc(W) : 0;
+      slot = __shfl_sync(kFull, slot, 0);
+    }
+    uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+    int capC = W.sl.capC;
+    int32_t* sp = nullptr;
+    if (slot >= 0) {
+      sp = W.slots + (size_t)slot * kSlotWords;
+      capC = (ncand + 31) & ~31;
+      masks = reinterpret_cast<uint32_t*>(sp + kSlotMasks);
+      subkey = reinterpret_cast<uint64_t*>(sp + kSlotMasks + K * capC);
+      uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
+      for (int b = lane; b < n; b += 32) lk[b] = lkey[b];
+    }
     for (int b0 = 0; b0 < nt; b0 += 32) {
       int q = b0 + lane;
       int p = q < nt ? tl[q] : 0;
@@ -566,9 +755,9 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       np += __popc(bp);
     }
     __syncwarp();
-    clear_masks(W, n, ncand);
-    uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
-    const int capC = W.sl.capC;
+    for (int w = 0; w < K; ++w)
+      for (int i = lane; i < ncand; i += 32) masks[(size_t)w * capC + i] = 0u;
+    __syncwarp();
     flat_rows(
         n,
         [&](int r, int& beg, int& len) {
@@ -584,7 +773,23 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
           if (si >= 0) atomicOr(&masks[(size_t)(r >> 5) * capC + si], 1u << (r & 31));
         });
     __syncwarp();
-    tier2(W, n, ncand, nq, sR, nR);
+    if (slot >= 0) {
+      if (lane == 0) {
+        sp[0] = K;
+        sp[1] = ncand;
+        sp[2] = nq;
+        sp[3] = capC;
+        for (int w = 0; w < 4; ++w) {
+          int bits = n - 32 * w;
+          sp[4 + w] = (int32_t)(bits >= 32 ? 0xffffffffu : (bits <= 0 ? 0u : ((1u << bits) - 1u)));
+        }
+        *reinterpret_cast<uint64_t*>(sp + 8) = sR;
+        sp[10] = (int32_t)nR;
+      }
+      if (!slot_publish(W, slot)) tier2_from_slot(W, slot);  // ring full: run it here
+    } else {
+      tier2(W, n, ncand, nq, sR, nR);
+    }
   }
   __syncwarp();
   // state after finder_pop(x, level), then clear the child scratch
@@ -813,6 +1018,43 @@ __device__ bool queue_push_children(Warp& W, const Task& t, int k, int nq, int n
   }
   __syncwarp();
   return true;
+}
+
+// Pushes one task (lane-uniform); false if the ring is full.
+__device__ bool queue_push_one(Warp& W, const Task& t) {
+  const int lane = (int)lane_id();
+  EnumCtl* ctl = W.ctl;
+  const int cap = W.p.queue_cap;
+  int ok = 0;
+  if (lane == 0) {
+    unsigned long long used = atomicAdd(&ctl->q_used, 1ULL);
+    if (used + 1 > (unsigned long long)cap) {
+      atomicAdd(&ctl->q_used, (unsigned long long)-1LL);
+    } else {
+      atomicAdd(&ctl->pending, 1ULL);
+      unsigned long long gp = atomicAdd(&ctl->q_tail, 1ULL);
+      unsigned long long slot = gp % (unsigned long long)cap;
+      volatile unsigned long long* st = W.q_seq + slot;
+      const unsigned long long free_tag = slot_free_tag(gp, cap);
+      int64_t spins = 0;
+      ok = 1;
+      while (*st != free_tag) {
+        if (++spins > W.p.slot_spin_limit) {
+          set_status(ctl, kStQueue, gp);
+          ok = 2;
+          break;
+        }
+        __nanosleep(64);
+      }
+      if (ok == 1) {
+        W.q_tasks[slot] = t;
+        __threadfence();
+        atomicExch(W.q_seq + slot, free_tag + 1);
+      }
+    }
+  }
+  ok = __shfl_sync(kFull, ok, 0);
+  return ok != 0;  // 2: the run is aborting; the task counts as handed over
 }
 
 // ---------------------------------------------------------------------------
@@ -1047,7 +1289,7 @@ __device__ void run_task(Warp& W, const Task& t) {
   }
   bool done = nL <= 1 || np == 0;
   // ---- split (src/IterFinderGpu.cu:835-858) ----
-  if (!done && k < 4) {
+  if (!done && k < 4 && W.p.vertex_split) {
     long long rest = np;
     if ((rest > W.p.bound_height || nL > W.p.bound_height) &&
         rest * (long long)nL > (long long)W.p.bound_size) {
@@ -1147,7 +1389,10 @@ __device__ void run_task(Warp& W, const Task& t) {
       t1.nq = nq;
       t1.sRtask = sR;
       t1.nRtask = nR;
+      uint64_t t1s = globaltimer_ns();
+      uint64_t t2_before = W.ns_t2;
       tier1_run(W, t1);
+      W.ns_t1 += (globaltimer_ns() - t1s) - (W.ns_t2 - t2_before);
     }
   }
   __syncwarp();
@@ -1160,7 +1405,8 @@ __device__ void run_task(Warp& W, const Task& t) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kEnumThreads, 1)
     mbe_enum_kernel(DevGraph g, EnumParams p, ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
-                    unsigned long long* q_seq, int32_t* scratch, unsigned long long* exit_ns) {
+                    unsigned long long* q_seq, SlotPool pool, int32_t* scratch,
+                    unsigned long long* exit_ns) {
   uint64_t t_start = globaltimer_ns();
   const int lane = (int)lane_id();
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1171,11 +1417,16 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   W.ctl = ctl;
   W.q_tasks = q_tasks;
   W.q_seq = q_seq;
+  W.slots = pool.slots;
+  W.slot_bits = pool.bits;
+  W.nslot = pool.nslot;
   W.base = scratch + (size_t)warp_global * (size_t)sl.words_per_warp;
   W.cnt = W.hash = W.nonmax = W.splits = 0;
+  W.ns_t1 = W.ns_t2 = W.n_t2 = 0;
+  uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0;
   const int nroots = g.n_roots;
   uint64_t idle_since = 0;
-  uint64_t busy_ns = 0, last_done_ns = 0;
+  uint64_t busy_ns = 0, last_done_ns = 0, idle_last = 0;
   while (true) {
     int ab = lane == 0 ? *(volatile int32_t*)&ctl->abort : 0;
     if (__shfl_sync(kFull, ab, 0)) break;
@@ -1199,12 +1450,20 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     if (have) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) t.v[i] = __shfl_sync(kFull, t.v[i], 0);
+      if (idle_since != 0 && lane == 0) atomicSub(&ctl->idle_warps, 1);
       uint64_t tb = globaltimer_ns();
-      run_task(W, t);
+      if (t.v[0] >= 0) run_task(W, t);
+      else tier2_from_slot(W, -2 - t.v[0]);  // an exported bitmap sub-problem
       __syncwarp();
       uint64_t te = globaltimer_ns();
       busy_ns += te - tb;
       last_done_ns = te - t_start;
+      ++n_tasks;
+      if (te - tb > max_task) {
+        max_task = te - tb;
+        int nl = t.v[0] >= 0 ? g.row_off[t.v[0] + 1] - g.row_off[t.v[0]] : 0;
+        max_info = ((unsigned long long)(unsigned)t.v[0] << 32) | (unsigned)nl;
+      }
       if (lane == 0) {
         __threadfence();
         atomicAdd(&ctl->pending, (unsigned long long)-1LL);
@@ -1222,8 +1481,11 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     finished = __shfl_sync(kFull, finished, 0);
     if (finished) break;
     uint64_t now = globaltimer_ns();
+    if (idle_since != 0) ns_idle += now - idle_last;
+    idle_last = now;
     if (idle_since == 0) {
       idle_since = now;
+      if (lane == 0) atomicAdd(&ctl->idle_warps, 1);
     } else if (now - idle_since > (uint64_t)p.idle_ns_limit) {
       if (lane == 0) set_status(ctl, kStTimeout, now - idle_since);
       break;
@@ -1236,6 +1498,14 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     if (W.hash) atomicAdd(&ctl->hash, W.hash);
     if (W.nonmax) atomicAdd(&ctl->non_maximal, W.nonmax);
     if (W.splits) atomicAdd(&ctl->tasks_split, W.splits);
+    atomicAdd(&ctl->ns_setup, (unsigned long long)(busy_ns - W.ns_t1 - W.ns_t2));
+    atomicAdd(&ctl->ns_tier1, (unsigned long long)W.ns_t1);
+    atomicAdd(&ctl->ns_tier2, (unsigned long long)W.ns_t2);
+    atomicAdd(&ctl->ns_idle, (unsigned long long)ns_idle);
+    atomicAdd(&ctl->n_tasks, (unsigned long long)n_tasks);
+    atomicAdd(&ctl->n_tier2, (unsigned long long)W.n_t2);
+    unsigned long long old = atomicMax(&ctl->max_task_ns, (unsigned long long)max_task);
+    if (old < max_task) atomicExch(&ctl->max_task_info, (unsigned long long)max_info);
   }
   if (p.record_exit) {
     // Per block: when its last task finished, and its warps' summed busy time.

@@ -196,7 +196,13 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
   ep.record_exit = 0;
   ep.tier2_max_l = t2;
-  mbe_enum_kernel<<<blocks, kEnumThreads, 0, st>>>(dg, ep, sl, ctl, q_tasks, q_seq, scratch, exit_ns);
+  SlotPool none;
+  none.slots = nullptr;
+  none.bits = nullptr;
+  none.nslot = 0;  // no sub-problem export out of the static pool
+  ep.vertex_split = 1;
+  mbe_enum_kernel<<<blocks, kEnumThreads, 0, st>>>(dg, ep, sl, ctl, q_tasks, q_seq, none, scratch,
+                                                   exit_ns);
   noalloc_finish<<<1, 32, 0, st>>>(ctl, d_out);
   if ((e = cudaGetLastError()) != cudaSuccess)
     return set_error(MBE_ERR_CUDA, "launch: %s", cudaGetErrorString(e));

@@ -88,6 +88,10 @@ typedef struct mbe_params {
   int32_t root_end;        /*   order (0, 0 = all); the internal order is -t/-o applied   */
   int32_t shard_count;     /* 0/1 = every root of the range; n > 1 = only the roots at     */
   int32_t shard_index;     /*   positions p = shard_index mod n, counted from the top      */
+  int32_t split_mode;      /* how a task passing the split test is shared out:             */
+                           /*   0 = its children's bitmap sub-problems go to idle warps     */
+                           /*   1 = GMBE's vertex-tuple child tasks (src/IterFinderGpu.cu:835-910) */
+  int32_t reserved;
 } mbe_params;
 
 typedef struct mbe_result {
@@ -101,6 +105,12 @@ typedef struct mbe_result {
   double sm_exit_max_ms; /* -p: latest time a block finished its last task, ms after launch */
   double sm_exit_min_ms; /* -p: earliest such time (max - min = load-balance skew) */
   double warp_busy_frac; /* -p: share of warp-time spent inside tasks */
+  /* Summed warp-time (ms) by phase: task set-up, counts tier, bitmap tier,
+   * idle waiting; the longest single task (ms), its root (internal id) and
+   * that root's |N(v)|; tasks run and bitmap sub-problems solved. */
+  double setup_ms, tier1_ms, tier2_ms, idle_ms, max_task_ms;
+  int32_t max_task_root, max_task_degree;
+  uint64_t n_tasks, n_subproblems;
 } mbe_result;
 
 /* Default parameters: bound_height 20, bound_size 1500, prune 1. */
