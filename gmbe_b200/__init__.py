@@ -57,7 +57,7 @@ class Params(C.Structure):
                 ("bitmap_max_l", C.c_int32), ("wait_limit_ns", C.c_int64),
                 ("sm_timing", C.c_int32), ("root_begin", C.c_int32), ("root_end", C.c_int32),
                 ("shard_count", C.c_int32), ("shard_index", C.c_int32),
-                ("split_mode", C.c_int32), ("reserved", C.c_int32)]
+                ("split_mode", C.c_int32), ("direct_max_c", C.c_int32)]
 
 
 class Result(C.Structure):

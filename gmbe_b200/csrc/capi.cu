@@ -177,21 +177,21 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   s.lsize = take(Lc + 2);
   s.aadj = take(S);
   s.cadj = take(S);
-  s.masks = take((int64_t)kKMax * C);
+  s.masks = take((int64_t)(kKMax + 1) * C);  // bitmap-tier records (K+1 words each)
   s.sub_v = take(2 * C);
   s.bound2 = take(C);
   s.lkey = take(2 * T2);
-  s.lmask = take((T2 + 2) * kKMax);
-  s.cursor2 = take(T2 + 2);
-  s.act_off = take(T2 + 2);
-  s.act_len = take(T2 + 2);
-  s.act_top = take(T2 + 2);
-  s.r_sum = take(2 * (T2 + 2));
-  s.r_cnt = take(T2 + 2);
+  s.lmask = take((T2 + 3) * kKMax);
+  s.t2_rec = take(2 * (T2 + 3));
+  s.t2_n = take(T2 + 3);
+  s.t2_cur = take(T2 + 3);
+  s.t2_top = take(T2 + 3);
+  s.r_sum = take(2 * (T2 + 3));
+  s.r_cnt = take(T2 + 3);
   s.tlist = take(C);
-  // Active-list arena of the bitmap tier: the level-1 list plus room for
-  // compacted deeper lists (a level that does not fit shares its parent's).
-  s.act_cap = (int32_t)std::min<int64_t>(INT32_MAX / 2, 3 * C + 4096);
+  // Arena of the bitmap tier's per-level record lists (a level that does not
+  // fit shares its parent's list).
+  s.act_cap = (int32_t)std::min<int64_t>(INT32_MAX / 2, 6 * C + 8192);
   s.act = take(s.act_cap);
   s.words_per_warp = off;
   return s;
@@ -311,6 +311,8 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   int blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * occ) : dev_sms * occ;
   const int warps = blocks * kEnumWarps;
   int32_t capC = std::max<int32_t>(1, std::min<int32_t>(h.V_size, g->capS));
+  if (capC >= (1 << 24))
+    return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
   ScratchLayout sl = make_layout(h.V_size, capC, g->capL, g->capS);
   size_t need = (size_t)sl.words_per_warp * (size_t)warps * sizeof(int32_t);
   if (need > ws.scratch_bytes) {
@@ -388,6 +390,7 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
   ep.record_exit = prm.sm_timing ? 1 : 0;
   ep.tier2_max_l = t2;
+  ep.direct_max_c = prm.direct_max_c > 0 ? prm.direct_max_c : 4096;
 
   CK(cudaEventRecord(ws.ev0));
   SlotPool pool;

@@ -69,8 +69,9 @@ struct ScratchLayout {
   int64_t lv, llevel, lp, aoff, stack, lsize;
   int64_t aadj, cadj;
   int64_t masks, sub_v, bound2;
-  int64_t lkey, lmask, cursor2;  // lkey is uint64 (8-byte aligned offset)
-  int64_t act, act_off, act_len, act_top, tlist, r_sum, r_cnt;  // r_sum is uint64
+  int64_t lkey, lmask;  // lkey is uint64 (8-byte aligned offset)
+  int64_t t2_rec, t2_n, t2_cur, t2_top, r_sum, r_cnt;  // bitmap-tier stack; t2_rec, r_sum uint64
+  int64_t act, tlist;
   int32_t act_cap, pad;
 };
 
@@ -89,7 +90,7 @@ struct EnumParams {
   int32_t record_exit;        // -p
   int32_t tier2_max_l;        // |L| at or below which the bitmap tier runs (<= 32*kmax)
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
-  int32_t pad;
+  int32_t direct_max_c;       // bitmap tier straight from set-up only while |C| <= this
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

@@ -74,9 +74,10 @@ __device__ __forceinline__ void flat_rows(int nr, RowOf row_of, Visit visit) {
 }
 
 struct Warp {
-  DevGraph g;
-  EnumParams p;
-  ScratchLayout sl;
+  // Launch constants, read in place from the kernel's parameter space.
+  const DevGraph& g;
+  const EnumParams& p;
+  const ScratchLayout& sl;
   EnumCtl* ctl;
   Task* q_tasks;
   unsigned long long* q_seq;
@@ -94,27 +95,39 @@ struct Warp {
 };
 
 // ---------------------------------------------------------------------------
-// Bitmap sub-problems and their export to idle warps.
+// Bitmap sub-problems.
+//
+// A sub-problem is an L of at most 128 vertices (K = 1, 2 or 4 words) and a
+// list of candidate records of K+1 words: word 0 = (index << 8) | bound,
+// words 1..K = the candidate's neighbourhood inside L.  index is the
+// candidate's position in the sub-problem, whose order is [Q | P]; bound is
+// GMBE's level bound in 8 bits (kB8Free = live at every level; levels stay
+// at or below 129).  subkey[index] is the candidate's hash key, lkey[b] that
+// of L bit b.
+constexpr uint32_t kB8Free = 255;
+
 struct T2Src {
-  const uint32_t* masks;  // masks[w * stride + i]: word w of candidate i inside L
-  int stride;
-  const uint64_t* subkey;  // hash key of candidate i
-  const uint64_t* lkey;    // hash key of L bit b
+  uint32_t* rec;           // nsub records, writable (their bounds change)
+  const uint64_t* subkey;
+  const uint64_t* lkey;
   uint32_t L0[4];          // the sub-problem's L
-  int nsub, nq;            // candidates [0, nq) are Q, [nq, nsub) P
+  int nsub, nq;            // records [0, nq) are Q, [nq, nsub) P
   uint64_t sR0;            // R of the sub-problem's root biclique
   uint32_t nR0;
 };
 
-// Slot layout (int32 words): header, lkey (128 x uint64), masks (K x stride), subkey.
+// Slot layout (int32 words): header, lkey (128 x uint64), records, subkey.
 constexpr int kSlotWords = 16384;
 constexpr int kSlotHdr = 16;
 constexpr int kSlotLkey = kSlotHdr;
-constexpr int kSlotMasks = kSlotLkey + 2 * 32 * 4;
-__host__ __device__ constexpr int slot_stride_max(int K) {
-  return ((kSlotWords - kSlotMasks) / (K + 2)) & ~31;
+constexpr int kSlotRec = kSlotLkey + 2 * 32 * 4;
+__host__ __device__ constexpr int slot_cap(int K) {
+  return ((kSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
 }
-// header words: 0 K, 1 nsub, 2 nq, 3 stride, 4..7 L0, 8..9 sR0, 10 nR0
+// header words: 0 K, 1 nsub, 2 nq, 4..7 L0, 8..9 sR0, 10 nR0
+__device__ __forceinline__ uint64_t* slot_subkey(int32_t* sp, int K, int nsub) {
+  return reinterpret_cast<uint64_t*>(sp + kSlotRec + ((nsub * (K + 1) + 1) & ~1));
+}
 
 // Claims a free slot (lane 0); -1 if none.
 __device__ int slot_alloc(Warp& W) {
@@ -157,7 +170,7 @@ __device__ __forceinline__ bool big_enough(const Warp& W, int nP, int nL) {
          (long long)nP * nL > (long long)W.p.bound_size;
 }
 
-// Writes a slot header and enqueues it; frees the slot if the ring is full.
+// Enqueues a filled slot as a task; false if the ring is full.
 __device__ bool slot_publish(Warp& W, int slot) {
   __syncwarp();
   __threadfence();
@@ -167,109 +180,85 @@ __device__ bool slot_publish(Warp& W, int slot) {
   return queue_push_one(W, t);
 }
 
-// Exports the child (list of candidate indices `child`, Ln, base R) of a
-// first-level push of a bitmap sub-problem.  The child's candidates keep
-// their order, so its first nbefore entries are its Q part.
+__device__ void slot_header(int32_t* sp, int K, int nsub, int nq, const uint32_t* L0, uint64_t sR,
+                            uint64_t nR) {
+  sp[0] = K;
+  sp[1] = nsub;
+  sp[2] = nq;
+  for (int w = 0; w < 4; ++w) sp[4 + w] = w < K ? (int32_t)L0[w] : 0;
+  *reinterpret_cast<uint64_t*>(sp + 8) = sR;
+  sp[10] = (int32_t)nR;
+}
+
+// Exports the child of a first-level push of a bitmap sub-problem (its
+// records `child`, in order, the first nbefore of them Q) to an idle warp.
 template <int K>
-__device__ bool t2_try_export(Warp& W, const T2Src& src, const int* child, int nchild, int nbefore,
-                              const uint32_t* Ln, int kn, uint64_t sR, uint64_t nR) {
-  if (nchild > slot_stride_max(K) || !big_enough(W, nchild - nbefore, kn) || !export_wanted(W))
+__device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, int nchild,
+                              int nbefore, const uint32_t* Ln, int kn, uint64_t sR, uint64_t nR) {
+  if (nchild > slot_cap(K) || !big_enough(W, nchild - nbefore, kn) || !export_wanted(W))
     return false;
   const int lane = (int)lane_id();
   int slot = lane == 0 ? slot_alloc(W) : 0;
   slot = __shfl_sync(0xffffffffu, slot, 0);
   if (slot < 0) return false;
+  constexpr int RS = K + 1;
   int32_t* sp = W.slots + (size_t)slot * kSlotWords;
-  const int stride = (nchild + 31) & ~31;
-  uint32_t* m = reinterpret_cast<uint32_t*>(sp + kSlotMasks);
-  uint64_t* key = reinterpret_cast<uint64_t*>(sp + kSlotMasks + K * stride);
+  uint32_t* rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
+  uint64_t* key = slot_subkey(sp, K, nchild);
   uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
   for (int q = lane; q < nchild; q += 32) {
-    int i = child[q];
+    const uint32_t* c = child + (size_t)q * RS;
+    rec[(size_t)q * RS] = ((uint32_t)q << 8) | kB8Free;
 #pragma unroll
-    for (int w = 0; w < K; ++w) m[(size_t)w * stride + q] = src.masks[(size_t)w * src.stride + i];
-    key[q] = src.subkey[i];
+    for (int w = 0; w < K; ++w) rec[(size_t)q * RS + 1 + w] = c[1 + w];
+    key[q] = src.subkey[c[0] >> 8];
   }
   for (int b = lane; b < 32 * K; b += 32) lk[b] = src.lkey[b];
-  if (lane == 0) {
-    sp[0] = K;
-    sp[1] = nchild;
-    sp[2] = nbefore;
-    sp[3] = stride;
-    for (int w = 0; w < 4; ++w) sp[4 + w] = w < K ? (int32_t)Ln[w] : 0;
-    *reinterpret_cast<uint64_t*>(sp + 8) = sR;
-    sp[10] = (int32_t)nR;
-  }
-  (void)kn;
+  if (lane == 0) slot_header(sp, K, nchild, nbefore, Ln, sR, nR);
   if (slot_publish(W, slot)) return true;
   if (lane == 0) slot_free(W, slot);
   __syncwarp();
   return false;
 }
 
-__device__ void tier2_dispatch(Warp& W, const T2Src& src, int words);
-
-// Runs an exported sub-problem and releases its slot.
-__device__ void tier2_from_slot(Warp& W, int slot) {
-  const int32_t* sp = W.slots + (size_t)slot * kSlotWords;
-  T2Src src;
-  const int K = sp[0];
-  src.nsub = sp[1];
-  src.nq = sp[2];
-  src.stride = sp[3];
-  for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)sp[4 + w];
-  src.sR0 = *reinterpret_cast<const uint64_t*>(sp + 8);
-  src.nR0 = (uint32_t)sp[10];
-  src.lkey = reinterpret_cast<const uint64_t*>(sp + kSlotLkey);
-  src.masks = reinterpret_cast<const uint32_t*>(sp + kSlotMasks);
-  src.subkey = reinterpret_cast<const uint64_t*>(sp + kSlotMasks + K * src.stride);
-  tier2_dispatch(W, src, K);
-  __syncwarp();
-  if (lane_id() == 0) slot_free(W, slot);
-  __syncwarp();
-}
-
 // ---------------------------------------------------------------------------
-// Tier 2: bitmap DFS over a sub-problem with n <= 32*K vertices in L.
-//   masks[w*capC + i] : word w of candidate i's neighbourhood inside L
-//   subkey[i]         : hash key of candidate i
-//   candidates [0, nq) are Q (already excluded), [nq, nsub) are P.
-// Restates IterProcess / finder_push / finder_pop on bitmaps.  Each level
-// keeps an active list: the candidates that still meet the level's L and are
-// not yet absorbed or pruned (MBEA's shrinking P and Q), so deep levels scan
-// only what can still matter.  A level whose list does not fit the arena
-// shares its parent's list (a superset; the scans re-test the mask).
+// Tier 2: the DFS of IterProcess / finder_push / finder_pop on a bitmap
+// sub-problem.  Every level owns a contiguous record list: the candidates
+// that still meet the level's L and are neither absorbed nor retired
+// (MBEA's shrinking P and Q), copied with their masks so each pass is a
+// unit-stride sweep.  Level bounds live in the records: a deeper level only
+// changes its own copies, which is equivalent to GMBE's shared bound array
+// because a pop at a level re-derives every bound >= that level.  A child
+// list that does not fit the arena shares its parent's records (GMBE's
+// shared-array semantics for that pair of levels).  R of the push that
+// opened a level is carried on the stack: absorbed candidates leave the
+// lists but stay in every R below.
 template <int K>
 __device__ void tier2_run(Warp& W, const T2Src& src) {
+  constexpr int RS = K + 1;
   const int lane = (int)lane_id();
-  const int capC = src.stride;
-  const uint32_t* masks = src.masks;
   const uint64_t* subkey = src.subkey;
-  int32_t* bound = W.A(W.sl.bound2);
   const uint64_t* lkey = src.lkey;
-  const int nsub = src.nsub, nq = src.nq;
-  uint32_t* lmask = reinterpret_cast<uint32_t*>(W.A(W.sl.lmask));
-  int32_t* cursor = W.A(W.sl.cursor2);   // position inside the level's active list
-  int32_t* aoff = W.A(W.sl.act_off);     // level list start in the arena
-  int32_t* alen = W.A(W.sl.act_len);     // level list length
-  int32_t* atop = W.A(W.sl.act_top);     // first free arena word after the level
-  int32_t* act = W.A(W.sl.act);
+  uint32_t* arena = reinterpret_cast<uint32_t*>(W.A(W.sl.act));
   const int actcap = W.sl.act_cap;
-  const bool prune = W.p.prune != 0;
-  // R of the push that opened each level: candidates absorbed above a level
-  // are not in its list but still belong to every R below it.
+  uint64_t* lrec = W.A64(W.sl.t2_rec);   // record list of each level
+  int32_t* ln = W.A(W.sl.t2_n);          // its length
+  int32_t* lcur = W.A(W.sl.t2_cur);      // scan position in it
+  int32_t* ltop = W.A(W.sl.t2_top);      // first free arena word above it
+  uint32_t* lmask = reinterpret_cast<uint32_t*>(W.A(W.sl.lmask));
   uint64_t* rsum = W.A64(W.sl.r_sum);
   uint32_t* rcnt = reinterpret_cast<uint32_t*>(W.A(W.sl.r_cnt));
+  const bool prune = W.p.prune != 0;
 
-  for (int i = lane; i < nsub; i += 32) {
-    bound[i] = kFree;
-    act[i] = i;
+  for (int q = lane; q < src.nsub; q += 32) {
+    uint32_t h = src.rec[(size_t)q * RS];
+    src.rec[(size_t)q * RS] = (h & ~0xffu) | kB8Free;
   }
   if (lane == 0) {
-    cursor[0] = nq;  // level 1 lists every candidate in order; P starts at nq
-    aoff[0] = 0;
-    alen[0] = nsub;
-    atop[0] = nsub;
+    lrec[0] = reinterpret_cast<uint64_t>(src.rec);
+    ln[0] = src.nsub;
+    lcur[0] = src.nq;
+    ltop[0] = 0;
     rsum[0] = src.sR0;
     rcnt[0] = src.nR0;
   }
@@ -283,76 +272,80 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
   __syncwarp();
   int level = 1;
   while (level != 0) {
+    uint32_t* R = reinterpret_cast<uint32_t*>(lrec[level - 1]);
+    const int n = ln[level - 1];
     uint32_t Lm[K];
 #pragma unroll
     for (int w = 0; w < K; ++w) Lm[w] = lmask[(level - 1) * K + w];
-    const int* A = act + aoff[level - 1];
-    const int na = alen[level - 1];
-    int cur = -1, curpos = -1;
-    for (int b0 = cursor[level - 1]; b0 < na; b0 += 32) {
+    int cp = -1;
+    for (int b0 = lcur[level - 1]; b0 < n; b0 += 32) {
       int q = b0 + lane;
       bool ok = false;
-      int i = 0;
-      if (q < na) {
-        i = A[q];
-        if (bound[i] > level - 1) {
+      if (q < n) {
+        const uint32_t* r = R + (size_t)q * RS;
+        if ((int)(r[0] & 0xffu) > level - 1) {
           uint32_t any = 0;
 #pragma unroll
-          for (int w = 0; w < K; ++w) any |= masks[(size_t)w * capC + i] & Lm[w];
+          for (int w = 0; w < K; ++w) any |= r[1 + w] & Lm[w];
           ok = any != 0;
         }
       }
       unsigned bal = __ballot_sync(kFull, ok);
       if (bal) {
-        int src = __ffs(bal) - 1;
-        curpos = b0 + src;
-        cur = __shfl_sync(kFull, i, src);
+        cp = b0 + __ffs(bal) - 1;
         break;
       }
     }
-    if (cur >= 0) {
+    if (cp >= 0) {
       // ---- push (finder_push) ----
       uint32_t Ln[K];
       int kn = 0;
 #pragma unroll
       for (int w = 0; w < K; ++w) {
-        Ln[w] = Lm[w] & masks[(size_t)w * capC + cur];
+        Ln[w] = Lm[w] & R[(size_t)cp * RS + 1 + w];
         kn += __popc(Ln[w]);
       }
-      // Child list goes above everything the stack holds.
-      const int ctop = atop[level - 1];
-      const bool fits = ctop + na <= actcap;
+      const int ctop = ltop[level - 1];
+      const bool fits = ctop + n * RS <= actcap;
+      uint32_t* child = arena + ctop;
       bool ism = true;
       uint64_t sR = 0;
       unsigned long long nR = 0;
-      int nchild = 0, nbefore = 0;  // child list size; entries before cur in it
-      for (int b0 = 0; b0 < na; b0 += 32) {
+      int nchild = 0, nbefore = 0;
+      for (int b0 = 0; b0 < n; b0 += 32) {
         int q = b0 + lane;
         bool keep = false;
-        int i = 0;
-        if (q < na) {
-          i = A[q];
+        uint32_t h = 0, m[K];
+        if (q < n) {
+          uint32_t* r = R + (size_t)q * RS;
+          h = r[0];
           bool cover = true, meet = false;
 #pragma unroll
           for (int w = 0; w < K; ++w) {
-            uint32_t m = masks[(size_t)w * capC + i] & Ln[w];
-            cover &= m == Ln[w];
-            meet |= m != 0;
+            m[w] = r[1 + w];
+            uint32_t x = m[w] & Ln[w];
+            cover &= x == Ln[w];
+            meet |= x != 0;
           }
-          int b = bound[i];
+          int b = (int)(h & 0xffu);
           if (cover) {
-            sR += subkey[i];
+            sR += subkey[h >> 8];
             ++nR;
-            if (i < cur && b >= level) ism = false;
-            else if (b > level) bound[i] = level;
+            if (q < cp && b >= level) ism = false;
+            else if (b > level) r[0] = (h & ~0xffu) | (uint32_t)level;
           } else {
             keep = meet && b > level;
           }
         }
         unsigned bal = __ballot_sync(kFull, keep);
-        if (fits && keep) act[ctop + nchild + __popc(bal & lanemask_lt())] = i;
+        if (fits && keep) {
+          uint32_t* c = child + (size_t)(nchild + __popc(bal & lanemask_lt())) * RS;
+          c[0] = (h & ~0xffu) | kB8Free;
+#pragma unroll
+          for (int w = 0; w < K; ++w) c[1 + w] = m[w];
+        }
         nchild += __popc(bal);
-        nbefore += __popc(__ballot_sync(kFull, keep && i < cur));
+        nbefore += __popc(__ballot_sync(kFull, keep && q < cp));
       }
       ism = __all_sync(kFull, ism);
       sR = warp_sum(sR) + rsum[level - 1];
@@ -373,23 +366,22 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
       // warp instead (the state after the pop below does not depend on it).
       bool exported = false;
       if (ism && kn > 1 && nchild > 0 && fits && level == 1)
-        exported = t2_try_export<K>(W, src, act + ctop, nchild, nbefore, Ln, kn, sR, nR);
+        exported = t2_try_export<K>(W, src, child, nchild, nbefore, Ln, kn, sR, nR);
       if (ism && kn > 1 && nchild > 0 && !exported) {
         if (lane == 0) {
-          cursor[level - 1] = curpos;
-          // The child level takes candidates after cur (exe_stack[level] =
-          // cur + 1); lists are in index order, so skip the entries before it.
-          cursor[level] = fits ? nbefore : curpos + 1;
+          lcur[level - 1] = cp;
           rsum[level] = sR;
           rcnt[level] = (uint32_t)nR;
           if (fits) {
-            aoff[level] = ctop;
-            alen[level] = nchild;
-            atop[level] = ctop + nchild;
+            lrec[level] = reinterpret_cast<uint64_t>(child);
+            ln[level] = nchild;
+            lcur[level] = nbefore;  // the child takes candidates after cp
+            ltop[level] = ctop + nchild * RS;
           } else {
-            aoff[level] = aoff[level - 1];
-            alen[level] = na;
-            atop[level] = ctop;
+            lrec[level] = lrec[level - 1];
+            ln[level] = n;
+            lcur[level] = cp + 1;
+            ltop[level] = ctop;
           }
         }
         if (lane < K) {
@@ -403,34 +395,35 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
         ++level;
         continue;
       }
-      if (lane == 0) cursor[level - 1] = curpos + 1;
+      if (lane == 0) lcur[level - 1] = cp + 1;
     } else {
       --level;
       if (level == 0) break;
-      int cp = cursor[level - 1];
-      cur = act[aoff[level - 1] + cp];
+      cp = lcur[level - 1];
       __syncwarp();
-      if (lane == 0) cursor[level - 1] = cp + 1;
+      if (lane == 0) lcur[level - 1] = cp + 1;
     }
-    // ---- pop (finder_pop) of candidate `cur` at `level` ----
+    // ---- pop (finder_pop) of the candidate at position cp of `level` ----
     {
-      const int* A = act + aoff[level - 1];
-      const int na = alen[level - 1];
+      uint32_t* R2 = reinterpret_cast<uint32_t*>(lrec[level - 1]);
+      const int n2 = ln[level - 1];
       uint32_t rem[K];
 #pragma unroll
-      for (int w = 0; w < K; ++w) rem[w] = lmask[(level - 1) * K + w] & ~masks[(size_t)w * capC + cur];
-      for (int q = lane; q < na; q += 32) {
-        int i = A[q];
-        int b = bound[i];
+      for (int w = 0; w < K; ++w)
+        rem[w] = lmask[(level - 1) * K + w] & ~R2[(size_t)cp * RS + 1 + w];
+      for (int q = lane; q < n2; q += 32) {
+        uint32_t* r = R2 + (size_t)q * RS;
+        uint32_t h = r[0];
+        int b = (int)(h & 0xffu);
         if (b >= level) {
+          uint32_t nb = kB8Free;
           if (prune) {
             uint32_t t = 0;
 #pragma unroll
-            for (int w = 0; w < K; ++w) t |= masks[(size_t)w * capC + i] & rem[w];
-            bound[i] = (t != 0 || i == cur) ? kFree : level - 1;
-          } else {
-            bound[i] = kFree;
+            for (int w = 0; w < K; ++w) t |= r[1 + w] & rem[w];
+            nb = (t != 0 || q == cp) ? kB8Free : (uint32_t)(level - 1);
           }
+          r[0] = (h & ~0xffu) | nb;
         }
       }
     }
@@ -447,33 +440,60 @@ __device__ void tier2_dispatch(Warp& W, const T2Src& src, int words) {
   W.n_t2 += 1;
 }
 
-// Sub-problem built in the warp's own scratch over n L vertices (all bits set).
-__device__ void tier2(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
-  T2Src src;
-  src.masks = reinterpret_cast<const uint32_t*>(W.A(W.sl.masks));
-  src.stride = W.sl.capC;
-  src.subkey = W.A64(W.sl.sub_v);
-  src.lkey = W.A64(W.sl.lkey);
+__device__ __forceinline__ int words_k(int n) {
+  int w = (n + 31) >> 5;
+  return w <= 1 ? 1 : (w <= 2 ? 2 : 4);
+}
+
+__device__ __forceinline__ void full_mask(uint32_t* L0, int n) {
 #pragma unroll
   for (int w = 0; w < 4; ++w) {
     int bits = n - 32 * w;
-    src.L0[w] = bits >= 32 ? 0xffffffffu : (bits <= 0 ? 0u : ((1u << bits) - 1u));
+    L0[w] = bits >= 32 ? 0xffffffffu : (bits <= 0 ? 0u : ((1u << bits) - 1u));
   }
+}
+
+// Sub-problem built in the warp's own scratch over n L vertices (all bits).
+__device__ void tier2(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
+  T2Src src;
+  src.rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+  src.subkey = W.A64(W.sl.sub_v);
+  src.lkey = W.A64(W.sl.lkey);
+  full_mask(src.L0, n);
   src.nsub = nsub;
   src.nq = nq;
   src.sR0 = sR0;
   src.nR0 = (uint32_t)nR0;
-  tier2_dispatch(W, src, (n + 31) >> 5);
+  tier2_dispatch(W, src, words_k(n));
 }
 
-// Zeroes the masks of candidates [0, nsub) for n vertices.
-__device__ void clear_masks(Warp& W, int n, int nsub) {
+// Runs an exported sub-problem and releases its slot.
+__device__ void tier2_from_slot(Warp& W, int slot) {
+  int32_t* sp = W.slots + (size_t)slot * kSlotWords;
+  T2Src src;
+  const int K = sp[0];
+  src.nsub = sp[1];
+  src.nq = sp[2];
+  for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)sp[4 + w];
+  src.sR0 = *reinterpret_cast<const uint64_t*>(sp + 8);
+  src.nR0 = (uint32_t)sp[10];
+  src.lkey = reinterpret_cast<const uint64_t*>(sp + kSlotLkey);
+  src.rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
+  src.subkey = slot_subkey(sp, K, src.nsub);
+  tier2_dispatch(W, src, K);
+  __syncwarp();
+  if (lane_id() == 0) slot_free(W, slot);
+  __syncwarp();
+}
+
+// Zeroes nsub records of K+1 words, each with its index and a free bound.
+__device__ void init_records(uint32_t* rec, int K, int nsub) {
   const int lane = (int)lane_id();
-  int words = (n + 31) >> 5;
-  int kw = words <= 1 ? 1 : (words <= 2 ? 2 : 4);
-  uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
-  for (int w = 0; w < kw; ++w)
-    for (int i = lane; i < nsub; i += 32) masks[(size_t)w * W.sl.capC + i] = 0u;
+  const int RS = K + 1;
+  for (int q = lane; q < nsub; q += 32) {
+    rec[(size_t)q * RS] = ((uint32_t)q << 8) | kB8Free;
+    for (int w = 0; w < K; ++w) rec[(size_t)q * RS + 1 + w] = 0u;
+  }
   __syncwarp();
 }
 
@@ -597,9 +617,9 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
   }
   __syncwarp();
   if (nsub > 0) {
-    clear_masks(W, n, nsub);
-    uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
-    const int capC = W.sl.capC;
+    const int K = words_k(n), RS = K + 1;
+    uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+    init_records(rec, K, nsub);
     flat_rows(
         n,
         [&](int r, int& beg, int& len) {
@@ -612,7 +632,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
           int p = aadj[pos];
           if (p < 0) return;
           int s = sidx[p];
-          if (s >= 0) atomicOr(&masks[(size_t)(r >> 5) * capC + s], 1u << (r & 31));
+          if (s >= 0) atomicOr(&rec[(size_t)s * RS + 1 + (r >> 5)], 1u << (r & 31));
         });
     __syncwarp();
     tier2(W, n, nsub, nq, sR, nR);
@@ -718,21 +738,18 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   if (ism && kept > 1 && ncand > 0) {
     // Destination: an export slot when idle warps want work and the child is
     // big enough by GMBE's split test, else this warp's scratch.
-    const int words = (n + 31) >> 5;
-    const int K = words <= 1 ? 1 : (words <= 2 ? 2 : 4);
+    const int K = words_k(n), RS = K + 1;
     int slot = -1;
-    if (ncand <= slot_stride_max(K) && big_enough(W, ncand - nqc, n) && export_wanted(W)) {
+    if (ncand <= slot_cap(K) && big_enough(W, ncand - nqc, n) && export_wanted(W)) {
       slot = lane == 0 ? slot_alloc(W) : 0;
       slot = __shfl_sync(kFull, slot, 0);
     }
-    uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
-    int capC = W.sl.capC;
+    uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
     int32_t* sp = nullptr;
     if (slot >= 0) {
       sp = W.slots + (size_t)slot * kSlotWords;
-      capC = (ncand + 31) & ~31;
-      masks = reinterpret_cast<uint32_t*>(sp + kSlotMasks);
-      subkey = reinterpret_cast<uint64_t*>(sp + kSlotMasks + K * capC);
+      rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
+      subkey = slot_subkey(sp, K, ncand);
       uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
       for (int b = lane; b < n; b += 32) lk[b] = lkey[b];
     }
@@ -755,9 +772,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       np += __popc(bp);
     }
     __syncwarp();
-    for (int w = 0; w < K; ++w)
-      for (int i = lane; i < ncand; i += 32) masks[(size_t)w * capC + i] = 0u;
-    __syncwarp();
+    init_records(rec, K, ncand);
     flat_rows(
         n,
         [&](int r, int& beg, int& len) {
@@ -770,21 +785,14 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
           int p = aadj[pos];
           if (p < 0) return;
           int si = sidx[p];
-          if (si >= 0) atomicOr(&masks[(size_t)(r >> 5) * capC + si], 1u << (r & 31));
+          if (si >= 0) atomicOr(&rec[(size_t)si * RS + 1 + (r >> 5)], 1u << (r & 31));
         });
     __syncwarp();
     if (slot >= 0) {
       if (lane == 0) {
-        sp[0] = K;
-        sp[1] = ncand;
-        sp[2] = nq;
-        sp[3] = capC;
-        for (int w = 0; w < 4; ++w) {
-          int bits = n - 32 * w;
-          sp[4 + w] = (int32_t)(bits >= 32 ? 0xffffffffu : (bits <= 0 ? 0u : ((1u << bits) - 1u)));
-        }
-        *reinterpret_cast<uint64_t*>(sp + 8) = sR;
-        sp[10] = (int32_t)nR;
+        uint32_t L0[4];
+        full_mask(L0, n);
+        slot_header(sp, K, ncand, nq, L0, sR, nR);
       }
       if (!slot_publish(W, slot)) tier2_from_slot(W, slot);  // ring full: run it here
     } else {
@@ -1300,15 +1308,15 @@ __device__ void run_task(Warp& W, const Task& t) {
     }
   }
   if (!done) {
-    if (nL <= W.p.tier2_max_l) {
+    if (nL <= W.p.tier2_max_l && nC <= W.p.direct_max_c) {
       // ---- tier 2 directly: masks of every candidate over all of L ----
       uint64_t* lkey = W.A64(W.sl.lkey);
       uint64_t* subkey = W.A64(W.sl.sub_v);
       for (int l = lane; l < nL; l += 32) lkey[l] = g.ukey[L[l]];
       for (int i = lane; i < nC; i += 32) subkey[i] = g.vkey[cv[i]];
-      clear_masks(W, nL, nC);
-      uint32_t* masks = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
-      const int capC = W.sl.capC;
+      const int K = words_k(nL), RS = K + 1;
+      uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+      init_records(rec, K, nC);
       flat_rows(
           nL,
           [&](int r, int& beg, int& len) {
@@ -1319,7 +1327,7 @@ __device__ void run_task(Warp& W, const Task& t) {
           [&](bool valid, int r, int pos) {
             if (!valid) return;
             int p = map[__ldg(g.rev_col + pos)] - 1;
-            if (p >= 0) atomicOr(&masks[(size_t)(r >> 5) * capC + p], 1u << (r & 31));
+            if (p >= 0) atomicOr(&rec[(size_t)p * RS + 1 + (r >> 5)], 1u << (r & 31));
           });
       __syncwarp();
       tier2(W, nL, nC, nq, sR, nR);
@@ -1404,16 +1412,14 @@ __device__ void run_task(Warp& W, const Task& t) {
 
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kEnumThreads, 1)
-    mbe_enum_kernel(DevGraph g, EnumParams p, ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
+    mbe_enum_kernel(const __grid_constant__ DevGraph g, const __grid_constant__ EnumParams p,
+                    const __grid_constant__ ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
                     unsigned long long* q_seq, SlotPool pool, int32_t* scratch,
                     unsigned long long* exit_ns) {
   uint64_t t_start = globaltimer_ns();
   const int lane = (int)lane_id();
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  Warp W;
-  W.g = g;
-  W.p = p;
-  W.sl = sl;
+  Warp W{g, p, sl};
   W.ctl = ctl;
   W.q_tasks = q_tasks;
   W.q_seq = q_seq;

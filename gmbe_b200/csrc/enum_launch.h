@@ -11,7 +11,9 @@ constexpr int kEnumWarps = 16;                 // warps per block
 constexpr int kEnumThreads = kEnumWarps * 32;  // threads per block
 constexpr int kKMax = 4;                       // bitmap words of the tier-2 sub-problem
 
-__global__ void mbe_enum_kernel(DevGraph g, EnumParams p, ScratchLayout sl, EnumCtl* ctl,
+__global__ void mbe_enum_kernel(const __grid_constant__ DevGraph g,
+                                const __grid_constant__ EnumParams p,
+                                const __grid_constant__ ScratchLayout sl, EnumCtl* ctl,
                                 Task* q_tasks, unsigned long long* q_seq, SlotPool pool,
                                 int32_t* scratch, unsigned long long* exit_ns);
 

@@ -111,6 +111,8 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   int32_t capS = (int32_t)std::max<int64_t>(capS64, 1);
   int32_t capL = std::max(nU, 1);
   int32_t capC = std::max<int32_t>(1, std::min<int32_t>(nV, capS));
+  if (capC >= (1 << 24))
+    return set_error(MBE_ERR_CAPACITY, "graph too large for the no-allocation pool");
   ScratchLayout sl = make_layout(nV, capC, capL, capS);
 
   // Pool partition: control block, split ring, per-block timing, hash keys,
@@ -196,6 +198,7 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
   ep.record_exit = 0;
   ep.tier2_max_l = t2;
+  ep.direct_max_c = 1 << 30;  // bitmap tier straight from set-up whenever |L| allows
   SlotPool none;
   none.slots = nullptr;
   none.bits = nullptr;

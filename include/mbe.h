@@ -91,7 +91,9 @@ typedef struct mbe_params {
   int32_t split_mode;      /* how a task passing the split test is shared out:             */
                            /*   0 = its children's bitmap sub-problems go to idle warps     */
                            /*   1 = GMBE's vertex-tuple child tasks (src/IterFinderGpu.cu:835-910) */
-  int32_t reserved;
+  int32_t direct_max_c;    /* a task with |L| <= bitmap_max_l goes straight to the bitmap  */
+                           /*   tier only while |C| <= this (0 = 2048); larger candidate   */
+                           /*   sets go through the counts tier's sparse pushes            */
 } mbe_params;
 
 typedef struct mbe_result {
