@@ -92,7 +92,7 @@ typedef struct mbe_params {
                            /*   0 = its children's bitmap sub-problems go to idle warps     */
                            /*   1 = GMBE's vertex-tuple child tasks (src/IterFinderGpu.cu:835-910) */
   int32_t direct_max_c;    /* a task with |L| <= bitmap_max_l goes straight to the bitmap  */
-                           /*   tier only while |C| <= this (0 = 2048); larger candidate   */
+                           /*   tier only while |C| <= this (0 = 4096); larger candidate   */
                            /*   sets go through the counts tier's sparse pushes            */
 } mbe_params;
 
