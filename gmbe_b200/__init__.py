@@ -101,6 +101,16 @@ _sig = {
     "mbe_read_adj": (C.c_int, [C.c_char_p, C.POINTER(_P32), C.POINTER(_P32), _P32, _P32,
                                C.POINTER(C.c_int64)]),
     "mbe_free": (None, [C.c_void_p]),
+    "mbe_batch_from_csr": (C.c_int, [C.c_int32, C.POINTER(_P32), C.POINTER(_P32), _P32, _P32,
+                                     C.POINTER(C.c_int64), C.POINTER(Opts),
+                                     C.POINTER(C.c_void_p)]),
+    "mbe_batch_size": (C.c_int, [C.c_void_p]),
+    "mbe_batch_set_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Params)]),
+    "mbe_batch_get_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Params)]),
+    "mbe_batch_run": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result),
+                                C.POINTER(Result)]),
+    "mbe_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(Params), C.c_int32, _P32]),
+    "mbe_batch_free": (C.c_int, [C.c_void_p]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(_lib, _name)
@@ -177,6 +187,66 @@ class Graph:
     def free(self):
         if self._h and self._h.value:
             _lib.mbe_graph_free(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many graphs in one device arena, enumerated in one persistent launch
+    (captured in a CUDA graph on the first run, replayed after that)."""
+
+    def __init__(self, graphs, uvtrans=1, order=1, fast_mode=1, device=0):
+        self._keep = [(_i32(g.row_off), _i32(g.col)) for g in graphs]
+        n = len(graphs)
+        ros = (_P32 * n)(*[_ptr(r) for r, _ in self._keep])
+        cos = (_P32 * n)(*[_ptr(c) for _, c in self._keep])
+        nvs = (C.c_int32 * n)(*[g.nV for g in graphs])
+        nus = (C.c_int32 * n)(*[g.nU for g in graphs])
+        nes = (C.c_int64 * n)(*[g.nE for g in graphs])
+        opts = make_opts(uvtrans, order, fast_mode, device)
+        h = C.c_void_p()
+        _check(_lib.mbe_batch_from_csr(n, ros, cos, nvs, nus, nes, C.byref(opts), C.byref(h)))
+        self._h = h
+        self.n = n
+        self._keep = None
+
+    def run(self, **params):
+        """Returns (per-graph results, totals)."""
+        p = default_params(**params)
+        per = (Result * self.n)()
+        tot = Result()
+        _check(_lib.mbe_batch_run(self._h, C.byref(p), per, C.byref(tot)))
+        return list(per), tot
+
+    def set_tuning(self, index=-1, **params):
+        p = default_params(**params)
+        _check(_lib.mbe_batch_set_tuning(self._h, index, C.byref(p)))
+
+    def get_tuning(self, index):
+        p = Params()
+        _check(_lib.mbe_batch_get_tuning(self._h, index, C.byref(p)))
+        return p
+
+    def autotune(self, n_classes=4, **params):
+        p = default_params(**params)
+        chosen = (C.c_int32 * n_classes)()
+        _check(_lib.mbe_batch_autotune(self._h, C.byref(p), n_classes, chosen))
+        return list(chosen)
+
+    def free(self):
+        if self._h and self._h.value:
+            _lib.mbe_batch_free(self._h)
             self._h = C.c_void_p()
 
     def __enter__(self):

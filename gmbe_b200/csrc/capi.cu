@@ -8,8 +8,7 @@
 #include <cstring>
 #include <mutex>
 
-#include "enum_launch.h"
-#include "internal.h"
+#include "engine.h"
 
 using namespace gmbe;
 
@@ -39,10 +38,10 @@ int cuda_fail(cudaError_t e, const char* what) {
   return set_error(MBE_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define CK(call)                                                  \
-  do {                                                            \
-    cudaError_t _e = (call);                                      \
-    if (_e != cudaSuccess) return cuda_fail(_e, #call);           \
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
   } while (0)
 
 inline uint64_t fmix64_h(uint64_t k) {
@@ -65,28 +64,6 @@ void free_device(mbe_graph* g) {
   g->d_ukey = g->d_vkey = nullptr;
 }
 
-// Engine workspace, one per device, shared by every graph on that device
-// and reused across calls (grown on demand).  A call holds the device's
-// workspace for its whole duration.
-struct Workspace {
-  std::mutex mu;
-  int32_t* scratch = nullptr;
-  size_t scratch_bytes = 0;
-  EnumCtl* ctl = nullptr;
-  Task* q_tasks = nullptr;
-  unsigned long long* q_seq = nullptr;
-  int32_t q_cap = 0;
-  unsigned long long* exit_ns = nullptr;
-  int32_t exit_cap = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int32_t* slots = nullptr;  // exported bitmap sub-problems
-  uint32_t* slot_bits = nullptr;
-  int32_t nslot = 0;
-  // Layout the per-warp count maps were last cleared for.
-  int64_t map_pitch_words = -1, map_words = -1;
-  int32_t map_warps = -1;
-};
-
 constexpr int kMaxDevices = 64;
 Workspace g_ws[kMaxDevices];
 
@@ -106,33 +83,14 @@ int upload_graph(mbe_graph* g) {
   if ((rc = upload(&g->d_col, h.col))) return rc;
   if ((rc = upload(&g->d_rev_off, h.rev_off))) return rc;
   if ((rc = upload(&g->d_rev_col, h.rev_col))) return rc;
-  // Hash keys in original ids and original sides (see include/mbe.h).
-  std::vector<uint64_t> uk(h.U_size), vk(h.V_size);
-  for (int32_t u = 0; u < h.U_size; ++u)
-    uk[u] = fmix64_h((uint64_t)h.u_orig[u] * 2u + (h.swapped ? 1u : 0u));
-  for (int32_t v = 0; v < h.V_size; ++v)
-    vk[v] = fmix64_h((uint64_t)h.v_orig[v] * 2u + (h.swapped ? 0u : 1u));
+  std::vector<uint64_t> uk, vk;
+  host_keys(h, &uk, &vk);
   if ((rc = upload(&g->d_ukey, uk))) return rc;
   if ((rc = upload(&g->d_vkey, vk))) return rc;
-  // Capacities: max over roots of |N(v)| and of sum_{u in N(v)} d(u).
-  int64_t capS = 0;
-  int32_t capL = 0;
-  for (int32_t v = 0; v < h.V_size; ++v) {
-    int64_t s = 0;
-    for (int32_t i = h.row_off[v]; i < h.row_off[v + 1]; ++i) {
-      int32_t u = h.col[i];
-      s += h.rev_off[u + 1] - h.rev_off[u];
-    }
-    capS = std::max(capS, s);
-    capL = std::max(capL, h.row_off[v + 1] - h.row_off[v]);
-  }
-  if (capS > INT32_MAX / 2) return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
-  g->capS = (int32_t)std::max<int64_t>(capS, 1);
-  g->capL = std::max(capL, 1);
-  return MBE_OK;
+  return graph_caps(h, &g->capL, &g->capS);
 }
 
-int finish_graph(mbe_graph* g, const mbe_opts& o, mbe_graph** out) {
+int finish_graph(mbe_graph* g, mbe_graph** out) {
   int rc = upload_graph(g);
   if (rc) {
     free_device(g);
@@ -146,6 +104,37 @@ int finish_graph(mbe_graph* g, const mbe_opts& o, mbe_graph** out) {
 }  // namespace
 
 namespace gmbe {
+
+Workspace& workspace(int device) { return g_ws[device]; }
+
+void host_keys(const HostGraph& h, std::vector<uint64_t>* uk, std::vector<uint64_t>* vk) {
+  // Keys in original ids and original sides (see include/mbe.h).
+  uk->resize(h.U_size);
+  vk->resize(h.V_size);
+  for (int32_t u = 0; u < h.U_size; ++u)
+    (*uk)[u] = fmix64_h((uint64_t)h.u_orig[u] * 2u + (h.swapped ? 1u : 0u));
+  for (int32_t v = 0; v < h.V_size; ++v)
+    (*vk)[v] = fmix64_h((uint64_t)h.v_orig[v] * 2u + (h.swapped ? 0u : 1u));
+}
+
+int graph_caps(const HostGraph& h, int32_t* capL_out, int32_t* capS_out) {
+  int64_t capS = 0;
+  int32_t capL = 0;
+  for (int32_t v = 0; v < h.V_size; ++v) {
+    int64_t s = 0;
+    for (int32_t i = h.row_off[v]; i < h.row_off[v + 1]; ++i) {
+      int32_t u = h.col[i];
+      s += h.rev_off[u + 1] - h.rev_off[u];
+    }
+    capS = std::max(capS, s);
+    capL = std::max(capL, h.row_off[v + 1] - h.row_off[v]);
+  }
+  if (capS > INT32_MAX / 2)
+    return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
+  *capS_out = (int32_t)std::max<int64_t>(capS, 1);
+  *capL_out = std::max(capL, 1);
+  return MBE_OK;
+}
 
 ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) {
   ScratchLayout s;
@@ -197,6 +186,164 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   return s;
 }
 
+int apply_tuning(const mbe_params& prm, DevGraph* dg) {
+  int t2 = prm.bitmap_max_l;
+  if (t2 == 0) t2 = 32 * kKMax;
+  if (t2 < 0) t2 = 1;
+  if (t2 > 32 * kKMax) return set_error(MBE_ERR_INVALID, "bitmap_max_l > %d", 32 * kKMax);
+  dg->bound_height = prm.bound_height;
+  dg->bound_size = prm.bound_size;
+  dg->tier2_max_l = t2;
+  dg->direct_max_c = prm.direct_max_c > 0 ? prm.direct_max_c : 4096;
+  return MBE_OK;
+}
+
+int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm, LaunchPlan* plan) {
+  if (!ws.ev0) {
+    CK(cudaEventCreate(&ws.ev0));
+    CK(cudaEventCreate(&ws.ev1));
+  }
+  int dev_sms = 0;
+  CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, spec.device));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
+  if (occ < 1) return set_error(MBE_ERR_CUDA, "enumeration kernel cannot be resident");
+  plan->blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * occ) : dev_sms * occ;
+  plan->warps = plan->blocks * kEnumWarps;
+  if (spec.capC >= (1 << 24))
+    return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
+  plan->sl = make_layout(spec.map_words, spec.capC, spec.capL, spec.capS);
+  plan->map_words = spec.map_words;
+  size_t need = (size_t)plan->sl.words_per_warp * (size_t)plan->warps * sizeof(int32_t);
+  if (need > ws.scratch_bytes) {
+    cudaFree(ws.scratch);
+    ws.scratch = nullptr;
+    ws.scratch_bytes = 0;
+    cudaError_t e = cudaMalloc((void**)&ws.scratch, need);
+    if (e != cudaSuccess)
+      return set_error(MBE_ERR_NOMEM, "scratch of %.2f GB: %s", need / 1e9, cudaGetErrorString(e));
+    ws.scratch_bytes = need;
+    ws.map_pitch_words = -1;
+    ++ws.gen;
+  }
+  // Every task leaves its warp's dense count map all-zero.  A different
+  // layout puts the maps elsewhere: they are cleared (strided, maps only).
+  plan->clear_maps = ws.map_pitch_words != plan->sl.words_per_warp ||
+                     ws.map_words != spec.map_words || ws.map_warps < plan->warps;
+  int32_t qcap = prm.queue_capacity > 0
+                     ? prm.queue_capacity
+                     : (int32_t)std::min<int64_t>(1 << 22,
+                                                  std::max<int64_t>(1 << 16, 8LL * spec.map_words));
+  if (qcap != ws.q_cap) {
+    cudaFree(ws.q_tasks);
+    cudaFree(ws.q_seq);
+    ws.q_tasks = nullptr;
+    ws.q_seq = nullptr;
+    ws.q_cap = 0;
+    CK(cudaMalloc((void**)&ws.q_tasks, sizeof(Task) * (size_t)qcap));
+    CK(cudaMalloc((void**)&ws.q_seq, sizeof(unsigned long long) * (size_t)qcap));
+    ws.q_cap = qcap;
+    ++ws.gen;
+  }
+  if (!ws.ctl) {
+    CK(cudaMalloc((void**)&ws.ctl, sizeof(EnumCtl)));
+    ++ws.gen;
+  }
+  if (!ws.slots) {
+    const int32_t nslot = 4096;  // 4096 x 128 KiB = 512 MiB
+    CK(cudaMalloc((void**)&ws.slots, sizeof(int32_t) * (size_t)kSlotWordsHost * nslot));
+    CK(cudaMalloc((void**)&ws.slot_bits, sizeof(uint32_t) * (size_t)(nslot / 32)));
+    ws.nslot = nslot;
+    ++ws.gen;
+  }
+  if (plan->blocks > ws.exit_cap) {
+    cudaFree(ws.exit_ns);
+    ws.exit_ns = nullptr;
+    ws.exit_cap = 0;
+    CK(cudaMalloc((void**)&ws.exit_ns, 2 * sizeof(unsigned long long) * (size_t)plan->blocks));
+    ws.exit_cap = plan->blocks;
+    ++ws.gen;
+  }
+  if (!ws.d_graph1) {
+    CK(cudaMalloc((void**)&ws.d_graph1, sizeof(DevGraph)));
+    CK(cudaMalloc((void**)&ws.d_prefix1, 2 * sizeof(long long)));
+    CK(cudaMalloc((void**)&ws.d_gres1, 3 * sizeof(unsigned long long)));
+  }
+  EnumParams& ep = plan->ep;
+  memset(&ep, 0, sizeof(ep));
+  ep.prune = prm.prune;
+  ep.queue_cap = qcap;
+  ep.slot_spin_limit = 20000000;  // x ~64 ns sleeps: a claimed slot is written within microseconds
+  ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
+  ep.record_exit = prm.sm_timing ? 1 : 0;
+  ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
+  ep.n_graphs = spec.n_graphs;
+  plan->pool.slots = ws.slots;
+  plan->pool.bits = ws.slot_bits;
+  plan->pool.nslot = prm.split_mode == 1 ? 0 : ws.nslot;
+  return MBE_OK;
+}
+
+int engine_clear_maps(Workspace& ws, LaunchPlan* plan, cudaStream_t st) {
+  if (!plan->clear_maps) return MBE_OK;
+  CK(cudaMemset2DAsync(ws.scratch, (size_t)plan->sl.words_per_warp * sizeof(int32_t), 0,
+                       (size_t)std::max<int32_t>(plan->map_words, 1) * sizeof(int32_t),
+                       (size_t)plan->warps, st));
+  ws.map_pitch_words = plan->sl.words_per_warp;
+  ws.map_words = plan->map_words;
+  ws.map_warps = plan->warps;
+  plan->clear_maps = false;
+  return MBE_OK;
+}
+
+int engine_enqueue(Workspace& ws, LaunchPlan* plan, const DevGraph* d_graphs,
+                   const long long* d_prefix, unsigned long long* d_gres, int n_graphs,
+                   cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
+  int rc = engine_clear_maps(ws, plan, st);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(ws.ctl, 0, sizeof(EnumCtl), st));
+  CK(cudaMemsetAsync(ws.q_seq, 0, sizeof(unsigned long long) * (size_t)ws.q_cap, st));
+  CK(cudaMemsetAsync(ws.slot_bits, 0, sizeof(uint32_t) * (size_t)(ws.nslot / 32), st));
+  CK(cudaMemsetAsync(d_gres, 0, 3 * sizeof(unsigned long long) * (size_t)n_graphs, st));
+  if (ev0) CK(cudaEventRecord(ev0, st));
+  mbe_enum_kernel<<<plan->blocks, kEnumThreads, 0, st>>>(d_graphs, d_prefix, d_gres, plan->ep,
+                                                          plan->sl, ws.ctl, ws.q_tasks, ws.q_seq,
+                                                          plan->pool, ws.scratch, ws.exit_ns);
+  CK(cudaGetLastError());
+  if (ev1) CK(cudaEventRecord(ev1, st));
+  return MBE_OK;
+}
+
+int engine_status(Workspace& ws, const EnumCtl& ctl) {
+  if (ctl.status == 0) return MBE_OK;
+  // An aborted run leaves count maps dirty: clear them on the next call.
+  ws.map_pitch_words = -1;
+  switch (ctl.status) {
+    case kStTimeout:
+      return set_error(MBE_ERR_TIMEOUT, "device wait limit reached (idle %llu ns)", ctl.err_info);
+    case kStQueue:
+      return set_error(MBE_ERR_TIMEOUT, "split-queue slot %llu was never written", ctl.err_info);
+    case kStCapacity:
+      return set_error(MBE_ERR_CAPACITY, "scratch capacity exceeded (info 0x%llx)", ctl.err_info);
+    default:
+      return set_error(MBE_ERR_CUDA, "device status %d", ctl.status);
+  }
+}
+
+void fill_profile(const EnumCtl& ctl, mbe_result* out) {
+  out->tasks_split = ctl.tasks_split;
+  out->status = ctl.status;
+  out->setup_ms = ctl.ns_setup / 1e6;
+  out->tier1_ms = ctl.ns_tier1 / 1e6;
+  out->tier2_ms = ctl.ns_tier2 / 1e6;
+  out->idle_ms = ctl.ns_idle / 1e6;
+  out->max_task_ms = ctl.max_task_ns / 1e6;
+  out->max_task_root = (int32_t)(ctl.max_task_info >> 32);
+  out->max_task_degree = (int32_t)(ctl.max_task_info & 0xffffffffu);
+  out->n_tasks = ctl.n_tasks;
+  out->n_subproblems = ctl.n_tier2;
+}
+
 }  // namespace gmbe
 
 extern "C" {
@@ -215,8 +362,6 @@ void mbe_opts_default(mbe_opts* o) {
   o->order = 1;  // reference Option() default (src/BiGraph.h:17-21)
 }
 
-const char* mbe_last_error_string(void);
-
 int mbe_graph_from_csr(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t nU,
                        int64_t nE, const mbe_opts* opts, mbe_graph** out) {
   clear_error();
@@ -225,6 +370,7 @@ int mbe_graph_from_csr(const int32_t* row_off, const int32_t* col, int32_t nV, i
   mbe_opts o;
   if (opts) o = *opts;
   else mbe_opts_default(&o);
+  if (o.device < 0 || o.device >= kMaxDevices) return set_error(MBE_ERR_INVALID, "bad device");
   mbe_graph* g = new mbe_graph();
   g->opts = o;
   g->device = o.device;
@@ -233,7 +379,7 @@ int mbe_graph_from_csr(const int32_t* row_off, const int32_t* col, int32_t nV, i
     delete g;
     return rc;
   }
-  return finish_graph(g, o, out);
+  return finish_graph(g, out);
 }
 
 int mbe_graph_from_adj(const char* path, const mbe_opts* opts, mbe_graph** out) {
@@ -279,7 +425,6 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   if (params) prm = *params;
   else mbe_params_default(&prm);
   const double t0 = now_s();  // reference exe_time_ starts at Execute() (src/IterFinderGpu.cu:1096)
-  if (g->device < 0 || g->device >= kMaxDevices) return set_error(MBE_ERR_INVALID, "bad device");
   CK(cudaSetDevice(g->device));
   const HostGraph& h = g->h;
   int32_t rb = prm.root_begin, re = prm.root_end;
@@ -291,81 +436,9 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   if (si < 0 || si >= sc) return set_error(MBE_ERR_INVALID, "shard_index %d outside [0,%d)", si, sc);
   int32_t span = re - rb;
   int32_t n_roots = span > si ? (span - si + sc - 1) / sc : 0;
-  int t2 = prm.bitmap_max_l;
-  if (t2 == 0) t2 = 32 * kKMax;
-  if (t2 < 0) t2 = 1;
-  if (t2 > 32 * kKMax) return set_error(MBE_ERR_INVALID, "bitmap_max_l > %d", 32 * kKMax);
-
-  Workspace& ws = g_ws[g->device];
-  std::lock_guard<std::mutex> lock(ws.mu);
-  if (!ws.ev0) {
-    CK(cudaEventCreate(&ws.ev0));
-    CK(cudaEventCreate(&ws.ev1));
-  }
-  // ---- launch shape and workspace ----
-  int dev_sms = 0;
-  CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device));
-  int occ = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
-  if (occ < 1) return set_error(MBE_ERR_CUDA, "enumeration kernel cannot be resident");
-  int blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * occ) : dev_sms * occ;
-  const int warps = blocks * kEnumWarps;
-  int32_t capC = std::max<int32_t>(1, std::min<int32_t>(h.V_size, g->capS));
-  if (capC >= (1 << 24))
-    return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
-  ScratchLayout sl = make_layout(h.V_size, capC, g->capL, g->capS);
-  size_t need = (size_t)sl.words_per_warp * (size_t)warps * sizeof(int32_t);
-  if (need > ws.scratch_bytes) {
-    cudaFree(ws.scratch);
-    ws.scratch = nullptr;
-    ws.scratch_bytes = 0;
-    cudaError_t e = cudaMalloc((void**)&ws.scratch, need);
-    if (e != cudaSuccess)
-      return set_error(MBE_ERR_NOMEM, "scratch of %.2f GB: %s", need / 1e9, cudaGetErrorString(e));
-    ws.scratch_bytes = need;
-    ws.map_pitch_words = -1;
-  }
-  // Every task leaves its warp's dense count map all-zero.  A different
-  // layout puts the maps elsewhere: clear them (strided, maps only).
-  if (ws.map_pitch_words != sl.words_per_warp || ws.map_words != h.V_size || ws.map_warps < warps) {
-    CK(cudaMemset2DAsync(ws.scratch, (size_t)sl.words_per_warp * sizeof(int32_t), 0,
-                         (size_t)std::max<int32_t>(h.V_size, 1) * sizeof(int32_t), (size_t)warps));
-    ws.map_pitch_words = sl.words_per_warp;
-    ws.map_words = h.V_size;
-    ws.map_warps = warps;
-  }
-  int32_t qcap = prm.queue_capacity > 0
-                     ? prm.queue_capacity
-                     : (int32_t)std::min<int64_t>(1 << 22, std::max<int64_t>(1 << 16, 8LL * h.V_size));
-  if (qcap != ws.q_cap) {
-    cudaFree(ws.q_tasks);
-    cudaFree(ws.q_seq);
-    ws.q_tasks = nullptr;
-    ws.q_seq = nullptr;
-    ws.q_cap = 0;
-    CK(cudaMalloc((void**)&ws.q_tasks, sizeof(Task) * (size_t)qcap));
-    CK(cudaMalloc((void**)&ws.q_seq, sizeof(unsigned long long) * (size_t)qcap));
-    ws.q_cap = qcap;
-  }
-  if (!ws.ctl) CK(cudaMalloc((void**)&ws.ctl, sizeof(EnumCtl)));
-  if (!ws.slots) {
-    const int32_t nslot = 4096;  // 4096 x 64 KiB = 256 MiB
-    CK(cudaMalloc((void**)&ws.slots, sizeof(int32_t) * (size_t)kSlotWordsHost * nslot));
-    CK(cudaMalloc((void**)&ws.slot_bits, sizeof(uint32_t) * (size_t)(nslot / 32)));
-    ws.nslot = nslot;
-  }
-  CK(cudaMemsetAsync(ws.slot_bits, 0, sizeof(uint32_t) * (size_t)(ws.nslot / 32)));
-  if (blocks > ws.exit_cap) {
-    cudaFree(ws.exit_ns);
-    ws.exit_ns = nullptr;
-    ws.exit_cap = 0;
-    CK(cudaMalloc((void**)&ws.exit_ns, 2 * sizeof(unsigned long long) * (size_t)blocks));
-    ws.exit_cap = blocks;
-  }
-  CK(cudaMemsetAsync(ws.ctl, 0, sizeof(EnumCtl)));
-  CK(cudaMemsetAsync(ws.q_seq, 0, sizeof(unsigned long long) * (size_t)qcap));
 
   DevGraph dg;
+  memset(&dg, 0, sizeof(dg));
   dg.nV = h.V_size;
   dg.nU = h.U_size;
   dg.nE = h.edge_size;
@@ -380,48 +453,38 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   dg.root_offset = si;
   dg.root_stride = sc;
   dg.n_roots = n_roots;
-  EnumParams ep;
-  memset(&ep, 0, sizeof(ep));
-  ep.bound_height = prm.bound_height;
-  ep.bound_size = prm.bound_size;
-  ep.prune = prm.prune;
-  ep.queue_cap = qcap;
-  ep.slot_spin_limit = 20000000;  // x ~64 ns sleeps: a claimed slot is written within microseconds
-  ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
-  ep.record_exit = prm.sm_timing ? 1 : 0;
-  ep.tier2_max_l = t2;
-  ep.direct_max_c = prm.direct_max_c > 0 ? prm.direct_max_c : 4096;
+  int rc = apply_tuning(prm, &dg);
+  if (rc) return rc;
 
-  CK(cudaEventRecord(ws.ev0));
-  SlotPool pool;
-  pool.slots = ws.slots;
-  pool.bits = ws.slot_bits;
-  pool.nslot = prm.split_mode == 1 ? 0 : ws.nslot;
-  ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
-  mbe_enum_kernel<<<blocks, kEnumThreads>>>(dg, ep, sl, ws.ctl, ws.q_tasks, ws.q_seq, pool,
-                                            ws.scratch, ws.exit_ns);
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(ws.ev1));
+  Workspace& ws = g_ws[g->device];
+  std::lock_guard<std::mutex> lock(ws.mu);
+  LaunchSpec spec;
+  spec.device = g->device;
+  spec.map_words = std::max<int32_t>(h.V_size, 1);
+  spec.capC = std::max<int32_t>(1, std::min<int32_t>(h.V_size, g->capS));
+  spec.capL = g->capL;
+  spec.capS = g->capS;
+  spec.n_graphs = 1;
+  LaunchPlan plan;
+  if ((rc = engine_prepare(ws, spec, prm, &plan))) return rc;
+  long long prefix[2] = {0, n_roots};
+  CK(cudaMemcpyAsync(ws.d_graph1, &dg, sizeof(dg), cudaMemcpyHostToDevice, 0));
+  CK(cudaMemcpyAsync(ws.d_prefix1, prefix, sizeof(prefix), cudaMemcpyHostToDevice, 0));
+  if ((rc = engine_enqueue(ws, &plan, ws.d_graph1, ws.d_prefix1, ws.d_gres1, 1, 0, ws.ev0, ws.ev1)))
+    return rc;
   EnumCtl ctl;
+  unsigned long long gres[3];
   CK(cudaMemcpy(&ctl, ws.ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(gres, ws.d_gres1, sizeof(gres), cudaMemcpyDeviceToHost));
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, ws.ev0, ws.ev1));
-  out->count = ctl.count;
-  out->set_hash = ctl.hash;
-  out->non_maximal = ctl.non_maximal;
-  out->tasks_split = ctl.tasks_split;
+  out->count = gres[0];
+  out->set_hash = gres[1];
+  out->non_maximal = gres[2];
   out->kernel_ms = ms;
-  out->status = ctl.status;
-  out->setup_ms = ctl.ns_setup / 1e6;
-  out->tier1_ms = ctl.ns_tier1 / 1e6;
-  out->tier2_ms = ctl.ns_tier2 / 1e6;
-  out->idle_ms = ctl.ns_idle / 1e6;
-  out->max_task_ms = ctl.max_task_ns / 1e6;
-  out->max_task_root = (int32_t)(ctl.max_task_info >> 32);
-  out->max_task_degree = (int32_t)(ctl.max_task_info & 0xffffffffu);
-  out->n_tasks = ctl.n_tasks;
-  out->n_subproblems = ctl.n_tier2;
+  fill_profile(ctl, out);
   if (prm.sm_timing) {
+    const int blocks = plan.blocks;
     std::vector<unsigned long long> ex(2 * (size_t)blocks);
     CK(cudaMemcpy(ex.data(), ws.exit_ns, 2 * sizeof(unsigned long long) * blocks,
                   cudaMemcpyDeviceToHost));
@@ -430,24 +493,10 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
     out->sm_exit_max_ms = *mm.second / 1e6;
     double busy = 0;
     for (int b = 0; b < blocks; ++b) busy += (double)ex[blocks + b];
-    out->warp_busy_frac = ms > 0 ? busy / 1e6 / ((double)warps * ms) : 0.0;
+    out->warp_busy_frac = ms > 0 ? busy / 1e6 / ((double)plan.warps * ms) : 0.0;
   }
   out->enum_seconds = now_s() - t0;
-  if (ctl.status != 0) {
-    // An aborted run leaves count maps dirty: clear them for the next call.
-    ws.map_pitch_words = -1;
-    switch (ctl.status) {
-      case kStTimeout:
-        return set_error(MBE_ERR_TIMEOUT, "device wait limit reached (idle %llu ns)", ctl.err_info);
-      case kStQueue:
-        return set_error(MBE_ERR_TIMEOUT, "split-queue slot %llu was never written", ctl.err_info);
-      case kStCapacity:
-        return set_error(MBE_ERR_CAPACITY, "scratch capacity exceeded (info 0x%llx)", ctl.err_info);
-      default:
-        return set_error(MBE_ERR_CUDA, "device status %d", ctl.status);
-    }
-  }
-  return MBE_OK;
+  return engine_status(ws, ctl);
 }
 
 }  // extern "C"

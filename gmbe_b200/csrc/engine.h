@@ -1,0 +1,92 @@
+// Host-side launch engine shared by the single-graph and batched entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "enum_launch.h"
+#include "internal.h"
+
+namespace gmbe {
+
+// Engine workspace, one per device, shared by every graph and batch on that
+// device and reused across calls (grown on demand).  A call holds the
+// device's workspace for its whole duration.
+struct Workspace {
+  std::mutex mu;
+  int32_t* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  EnumCtl* ctl = nullptr;
+  Task* q_tasks = nullptr;
+  unsigned long long* q_seq = nullptr;
+  int32_t q_cap = 0;
+  unsigned long long* exit_ns = nullptr;
+  int32_t exit_cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int32_t* slots = nullptr;  // exported bitmap sub-problems
+  uint32_t* slot_bits = nullptr;
+  int32_t nslot = 0;
+  // Single-graph launch descriptors.
+  DevGraph* d_graph1 = nullptr;
+  long long* d_prefix1 = nullptr;
+  unsigned long long* d_gres1 = nullptr;
+  // Layout the per-warp count maps were last cleared for.
+  int64_t map_pitch_words = -1, map_words = -1;
+  int32_t map_warps = -1;
+  // Bumped whenever a buffer above is (re)allocated: a captured launch that
+  // refers to an older generation must be captured again.
+  uint64_t gen = 1;
+};
+
+Workspace& workspace(int device);
+
+// What one launch needs from the workspace: the largest internal V side (the
+// count maps) and the per-warp capacities, maxima over the launch's graphs.
+struct LaunchSpec {
+  int device = 0;
+  int32_t map_words = 1;
+  int32_t capC = 1, capL = 1, capS = 1;
+  int32_t n_graphs = 1;
+};
+
+struct LaunchPlan {
+  int blocks = 0, warps = 0;
+  ScratchLayout sl;
+  EnumParams ep;
+  SlotPool pool;
+  bool clear_maps = false;
+  int32_t map_words = 1;
+};
+
+// Allocates or grows the workspace and fixes the launch shape (host-only,
+// not capturable).  Caller holds ws.mu.
+int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm, LaunchPlan* plan);
+
+// Queues the strided clear of every warp's count map if the layout changed
+// since the maps were last cleared (capturable; a no-op otherwise).
+int engine_clear_maps(Workspace& ws, LaunchPlan* plan, cudaStream_t st);
+
+// Queues the launch: control-block, ring-tag, slot-map and result clears,
+// the count-map clear if the layout changed, and the kernel (capturable).
+// ev0/ev1, when given, bracket the kernel.
+int engine_enqueue(Workspace& ws, LaunchPlan* plan, const DevGraph* d_graphs,
+                   const long long* d_prefix, unsigned long long* d_gres, int n_graphs,
+                   cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
+
+// Status word -> MBE_ERR_* with a message; clears the count-map state.
+int engine_status(Workspace& ws, const EnumCtl& ctl);
+
+// Copies the profile counters of the control block into a result.
+void fill_profile(const EnumCtl& ctl, mbe_result* out);
+
+// Per-graph tuning fields of a descriptor from parameters.
+int apply_tuning(const mbe_params& prm, DevGraph* dg);
+
+// Hash keys (original ids, original sides) of an internal graph.
+void host_keys(const HostGraph& h, std::vector<uint64_t>* uk, std::vector<uint64_t>* vk);
+
+// Capacities of a graph: max |N(v)| and max sum_{u in N(v)} d(u) over roots.
+int graph_caps(const HostGraph& h, int32_t* capL, int32_t* capS);
+
+}  // namespace gmbe

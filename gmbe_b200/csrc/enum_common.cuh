@@ -27,12 +27,17 @@ struct DevGraph {
   // Roots: position p = 0 .. n_roots-1 is internal vertex
   // root_end - 1 - (root_offset + p * root_stride).
   int32_t root_end, root_offset, root_stride, n_roots;
+  // Per-graph tuning (results do not depend on it): GMBE's split bounds, the
+  // bitmap-tier limit on |L| and the direct-entry limit on |C|.
+  int32_t bound_height, bound_size, tier2_max_l, direct_max_c;
 };
 
 // A task: up to four internal V vertices, -1 padded (reference LongTask,
 // src/GpuUtil.cuh:394-462).  Roots are one-vertex tasks.
 struct alignas(16) Task {
   int32_t v[4];
+  int32_t graph;  // index into the launch's graph array
+  int32_t pad[3];
 };
 
 // Global control block (one per launch).
@@ -43,10 +48,11 @@ struct EnumCtl {
   unsigned long long non_maximal;
   unsigned long long tasks_split;
   // scheduling
-  int32_t next_root;     // roots handed out so far (descending internal id)
+  long long next_root;   // root positions handed out so far (all graphs of the launch)
   int32_t status;        // first error code
   int32_t abort;         // set together with status
   int32_t idle_warps;    // warps waiting for work (export demand)
+  int32_t pad0;
   unsigned long long pending;   // queued + running tasks (termination)
   unsigned long long q_head;    // next slot to consume
   unsigned long long q_tail;    // next slot to produce
@@ -77,20 +83,20 @@ struct ScratchLayout {
 
 // Slots for bitmap sub-problems handed to idle warps.
 struct SlotPool {
-  int32_t* slots;  // nslot x 16384 int32 words
+  int32_t* slots;  // nslot x 32768 int32 words
   uint32_t* bits;  // occupancy, nslot / 32 words, zero at launch
   int32_t nslot;   // multiple of 32; 0 disables export
 };
 
 struct EnumParams {
-  int32_t bound_height, bound_size, prune;
+  int32_t prune;
   int32_t queue_cap;
   int64_t slot_spin_limit;    // iterations waiting for a claimed slot to be written
   int64_t idle_ns_limit;      // nanoseconds a warp may idle waiting for work
   int32_t record_exit;        // -p
-  int32_t tier2_max_l;        // |L| at or below which the bitmap tier runs (<= 32*kmax)
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
-  int32_t direct_max_c;       // bitmap tier straight from set-up only while |C| <= this
+  int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)
+  int32_t pad;
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

@@ -75,7 +75,6 @@ __device__ __forceinline__ void flat_rows(int nr, RowOf row_of, Visit visit) {
 
 struct Warp {
   // Launch constants, read in place from the kernel's parameter space.
-  const DevGraph& g;
   const EnumParams& p;
   const ScratchLayout& sl;
   EnumCtl* ctl;
@@ -85,6 +84,9 @@ struct Warp {
   uint32_t* slot_bits;   // slot occupancy
   int nslot;
   int32_t* base;
+  const DevGraph* graphs;  // every graph of the launch
+  const DevGraph* gp;      // graph of the task being run
+  int32_t gid;
   // accumulators (uniform over lanes)
   unsigned long long cnt, hash, nonmax, splits;
   unsigned long long ns_t2, n_t2;  // time inside the bitmap tier, sub-problems run
@@ -117,14 +119,14 @@ struct T2Src {
 };
 
 // Slot layout (int32 words): header, lkey (128 x uint64), records, subkey.
-constexpr int kSlotWords = 16384;
+constexpr int kSlotWords = 32768;
 constexpr int kSlotHdr = 16;
 constexpr int kSlotLkey = kSlotHdr;
 constexpr int kSlotRec = kSlotLkey + 2 * 32 * 4;
 __host__ __device__ constexpr int slot_cap(int K) {
   return ((kSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
 }
-// header words: 0 K, 1 nsub, 2 nq, 4..7 L0, 8..9 sR0, 10 nR0
+// header words: 0 K, 1 nsub, 2 nq, 3 graph, 4..7 L0, 8..9 sR0, 10 nR0
 __device__ __forceinline__ uint64_t* slot_subkey(int32_t* sp, int K, int nsub) {
   return reinterpret_cast<uint64_t*>(sp + kSlotRec + ((nsub * (K + 1) + 1) & ~1));
 }
@@ -166,8 +168,8 @@ __device__ bool export_wanted(Warp& W) {
 
 // GMBE's split test on a child: (|P| > h or |L| > h) and |P| * |L| > s.
 __device__ __forceinline__ bool big_enough(const Warp& W, int nP, int nL) {
-  return (nP > W.p.bound_height || nL > W.p.bound_height) &&
-         (long long)nP * nL > (long long)W.p.bound_size;
+  return (nP > W.gp->bound_height || nL > W.gp->bound_height) &&
+         (long long)nP * nL > (long long)W.gp->bound_size;
 }
 
 // Enqueues a filled slot as a task; false if the ring is full.
@@ -181,17 +183,18 @@ __device__ bool slot_publish(Warp& W, int slot) {
 }
 
 __device__ void slot_header(int32_t* sp, int K, int nsub, int nq, const uint32_t* L0, uint64_t sR,
-                            uint64_t nR) {
+                            uint64_t nR, int gid) {
   sp[0] = K;
   sp[1] = nsub;
   sp[2] = nq;
+  sp[3] = gid;
   for (int w = 0; w < 4; ++w) sp[4 + w] = w < K ? (int32_t)L0[w] : 0;
   *reinterpret_cast<uint64_t*>(sp + 8) = sR;
   sp[10] = (int32_t)nR;
 }
 
-// Exports the child of a first-level push of a bitmap sub-problem (its
-// records `child`, in order, the first nbefore of them Q) to an idle warp.
+// Exports the child of a push of a bitmap sub-problem (its records
+// `child`, in order, the first nbefore of them Q) to an idle warp.
 template <int K>
 __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, int nchild,
                               int nbefore, const uint32_t* Ln, int kn, uint64_t sR, uint64_t nR) {
@@ -214,7 +217,7 @@ __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, 
     key[q] = src.subkey[c[0] >> 8];
   }
   for (int b = lane; b < 32 * K; b += 32) lk[b] = src.lkey[b];
-  if (lane == 0) slot_header(sp, K, nchild, nbefore, Ln, sR, nR);
+  if (lane == 0) slot_header(sp, K, nchild, nbefore, Ln, sR, nR, W.gid);
   if (slot_publish(W, slot)) return true;
   if (lane == 0) slot_free(W, slot);
   __syncwarp();
@@ -357,15 +360,16 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
           if ((Ln[w] >> lane) & 1u) sL += lkey[w * 32 + lane];
         sL = warp_sum(sL);
         W.cnt += 1;
-        W.hash += biclique_hash(W.g, sL, (uint64_t)kn, sR, nR);
+        W.hash += biclique_hash(*W.gp, sL, (uint64_t)kn, sR, nR);
       } else {
         W.nonmax += 1;
       }
       __syncwarp();
-      // A big enough child of the sub-problem's first level goes to an idle
-      // warp instead (the state after the pop below does not depend on it).
+      // A big enough child goes to an idle warp instead, at any depth, so a
+      // subtree that started inline can still be shared once warps run out of
+      // work (the state after the pop below does not depend on the child).
       bool exported = false;
-      if (ism && kn > 1 && nchild > 0 && fits && level == 1)
+      if (ism && kn > 1 && nchild > 0 && fits)
         exported = t2_try_export<K>(W, src, child, nchild, nbefore, Ln, kn, sR, nR);
       if (ism && kn > 1 && nchild > 0 && !exported) {
         if (lane == 0) {
@@ -474,6 +478,8 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   const int K = sp[0];
   src.nsub = sp[1];
   src.nq = sp[2];
+  W.gid = sp[3];
+  W.gp = W.graphs + W.gid;
   for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)sp[4 + w];
   src.sR0 = *reinterpret_cast<const uint64_t*>(sp + 8);
   src.nR0 = (uint32_t)sp[10];
@@ -590,7 +596,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
     if (sel) {
       int j = n + __popc(bal & lanemask_lt());
       lp[j] = l;
-      lkey[j] = W.g.ukey[t.L[l]];
+      lkey[j] = W.gp->ukey[t.L[l]];
     }
     n += __popc(bal);
   }
@@ -608,7 +614,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
     if (sel) {
       int s = nsub + __popc(bal & lanemask_lt());
       sidx[i] = s;
-      subkey[s] = W.g.vkey[cv[i]];
+      subkey[s] = W.gp->vkey[cv[i]];
     }
     nsub += __popc(bal);
     // candidates before x are Q
@@ -679,7 +685,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       if (sel) {
         int q = n + __popc(bal & lanemask_lt());
         lp[q] = l;
-        if (q < 32 * kKMax) lkey[q] = W.g.ukey[t.L[l]];
+        if (q < 32 * kKMax) lkey[q] = W.gp->ukey[t.L[l]];
       }
       n += __popc(bal);
     }
@@ -716,7 +722,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       p = tl[q];
       int c = cc[p];
       if (c == kept) {
-        sR += W.g.vkey[cv[p]];
+        sR += W.gp->vkey[cv[p]];
         ++nR;
         if (p < x && bound[p] >= level) ism = false;
       } else {
@@ -731,7 +737,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   nR = warp_sum(nR) + t.nRtask;
   if (ism) {
     W.cnt += 1;
-    W.hash += biclique_hash(W.g, sL, (uint64_t)kept, sR, nR);
+    W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
   } else {
     W.nonmax += 1;
   }
@@ -766,7 +772,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       if (isP) s = ncand - 1 - (np + __popc(bp & lanemask_lt()));
       if (s >= 0) {
         sidx[p] = s;
-        subkey[s] = W.g.vkey[cv[p]];
+        subkey[s] = W.gp->vkey[cv[p]];
       }
       nq += __popc(bq);
       np += __popc(bp);
@@ -792,7 +798,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       if (lane == 0) {
         uint32_t L0[4];
         full_mask(L0, n);
-        slot_header(sp, K, ncand, nq, L0, sR, nR);
+        slot_header(sp, K, ncand, nq, L0, sR, nR, W.gid);
       }
       if (!slot_publish(W, slot)) tier2_from_slot(W, slot);  // ring full: run it here
     } else {
@@ -822,7 +828,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
   const int32_t* coff = W.A(W.sl.coff);
   const int32_t* cadj = W.A(W.sl.cadj);
   const int32_t* aadj = W.A(W.sl.aadj);
-  const int t2max = W.p.tier2_max_l;
+  const int t2max = W.gp->tier2_max_l;
 
   if (lane == 0) {
     stack[0] = t.nq;
@@ -853,7 +859,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
         if (llevel[l] == level - 1) {
           llevel[l] = level;
           ++kept;
-          sL += W.g.ukey[t.L[l]];
+          sL += W.gp->ukey[t.L[l]];
         }
       }
       kept = warp_sum(kept);
@@ -888,7 +894,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       unsigned long long nR = 0;
       for (int i = lane; i < t.nC; i += 32) {
         if (ncnt[i] == kept) {
-          sR += W.g.vkey[cv[i]];
+          sR += W.gp->vkey[cv[i]];
           ++nR;
           int b = bound[i];
           if (i < cur && b >= level) ism = false;
@@ -900,7 +906,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       nR = warp_sum(nR) + t.nRtask;
       if (ism) {
         W.cnt += 1;
-        W.hash += biclique_hash(W.g, sL, (uint64_t)kept, sR, nR);
+        W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
       } else {
         W.nonmax += 1;
       }
@@ -974,6 +980,7 @@ __device__ bool queue_pop(Warp& W, Task* out) {
   out->v[1] = src[1];
   out->v[2] = src[2];
   out->v[3] = src[3];
+  out->graph = src[4];
   __threadfence();
   atomicExch(W.q_seq + slot, full + 1);  // free for round h/cap + 1
   atomicAdd(&ctl->q_used, (unsigned long long)-1LL);
@@ -1069,7 +1076,7 @@ __device__ bool queue_push_one(Warp& W, const Task& t) {
 // Task set-up (IterFinderWithMultipleVertex) and dispatch.
 __device__ void run_task(Warp& W, const Task& t) {
   const int lane = (int)lane_id();
-  const DevGraph& g = W.g;
+  const DevGraph& g = *W.gp;
   int k = 1;
   while (k < 4 && t.v[k] >= 0) ++k;
   const int last = t.v[k - 1];
@@ -1299,8 +1306,8 @@ __device__ void run_task(Warp& W, const Task& t) {
   // ---- split (src/IterFinderGpu.cu:835-858) ----
   if (!done && k < 4 && W.p.vertex_split) {
     long long rest = np;
-    if ((rest > W.p.bound_height || nL > W.p.bound_height) &&
-        rest * (long long)nL > (long long)W.p.bound_size) {
+    if ((rest > W.gp->bound_height || nL > W.gp->bound_height) &&
+        rest * (long long)nL > (long long)W.gp->bound_size) {
       if (queue_push_children(W, t, k, nq, nC)) {
         W.splits += 1;
         done = true;
@@ -1308,7 +1315,7 @@ __device__ void run_task(Warp& W, const Task& t) {
     }
   }
   if (!done) {
-    if (nL <= W.p.tier2_max_l && nC <= W.p.direct_max_c) {
+    if (nL <= W.gp->tier2_max_l && nC <= W.gp->direct_max_c) {
       // ---- tier 2 directly: masks of every candidate over all of L ----
       uint64_t* lkey = W.A64(W.sl.lkey);
       uint64_t* subkey = W.A64(W.sl.sub_v);
@@ -1411,15 +1418,28 @@ __device__ void run_task(Warp& W, const Task& t) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Maps a global root position to (graph, root vertex): positions are the
+// graphs' root lists laid end to end (root_prefix[i] = roots before graph i).
+__device__ __forceinline__ int graph_of_position(const long long* prefix, int n, long long pos) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= pos) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 __global__ void __launch_bounds__(kEnumThreads, 1)
-    mbe_enum_kernel(const __grid_constant__ DevGraph g, const __grid_constant__ EnumParams p,
+    mbe_enum_kernel(const DevGraph* graphs, const long long* root_prefix,
+                    unsigned long long* gres, const __grid_constant__ EnumParams p,
                     const __grid_constant__ ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
                     unsigned long long* q_seq, SlotPool pool, int32_t* scratch,
                     unsigned long long* exit_ns) {
   uint64_t t_start = globaltimer_ns();
   const int lane = (int)lane_id();
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  Warp W{g, p, sl};
+  Warp W{p, sl};
   W.ctl = ctl;
   W.q_tasks = q_tasks;
   W.q_seq = q_seq;
@@ -1427,10 +1447,13 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   W.slot_bits = pool.bits;
   W.nslot = pool.nslot;
   W.base = scratch + (size_t)warp_global * (size_t)sl.words_per_warp;
+  W.graphs = graphs;
+  W.gp = graphs;
+  W.gid = 0;
   W.cnt = W.hash = W.nonmax = W.splits = 0;
   W.ns_t1 = W.ns_t2 = W.n_t2 = 0;
   uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0;
-  const int nroots = g.n_roots;
+  const long long nroots = root_prefix[p.n_graphs];
   uint64_t idle_since = 0;
   uint64_t busy_ns = 0, last_done_ns = 0, idle_last = 0;
   while (true) {
@@ -1440,12 +1463,16 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     int have = 0;
     if (lane == 0) {
       have = queue_pop(W, &t) ? 1 : 0;
-      if (!have && *(volatile int32_t*)&ctl->next_root < nroots) {
+      if (!have && *(volatile long long*)&ctl->next_root < nroots) {
         atomicAdd(&ctl->pending, 1ULL);
-        int r = atomicAdd(&ctl->next_root, 1);
+        long long r = (long long)atomicAdd((unsigned long long*)&ctl->next_root, 1ULL);
         if (r < nroots) {
-          t.v[0] = g.root_end - 1 - (g.root_offset + r * g.root_stride);
+          int gi = graph_of_position(root_prefix, p.n_graphs, r);
+          const DevGraph& gg = graphs[gi];
+          long long k = r - root_prefix[gi];
+          t.v[0] = gg.root_end - 1 - (int)(gg.root_offset + k * gg.root_stride);
           t.v[1] = t.v[2] = t.v[3] = -1;
+          t.graph = gi;
           have = 1;
         } else {
           atomicAdd(&ctl->pending, (unsigned long long)-1LL);
@@ -1456,18 +1483,32 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     if (have) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) t.v[i] = __shfl_sync(kFull, t.v[i], 0);
+      t.graph = __shfl_sync(kFull, t.graph, 0);
       if (idle_since != 0 && lane == 0) atomicSub(&ctl->idle_warps, 1);
       uint64_t tb = globaltimer_ns();
-      if (t.v[0] >= 0) run_task(W, t);
-      else tier2_from_slot(W, -2 - t.v[0]);  // an exported bitmap sub-problem
+      if (t.v[0] >= 0) {
+        W.gid = t.graph;
+        W.gp = graphs + t.graph;
+        run_task(W, t);
+      } else {
+        tier2_from_slot(W, -2 - t.v[0]);  // an exported bitmap sub-problem (sets the graph)
+      }
       __syncwarp();
+      // Results go to the task's graph.
+      if (lane == 0) {
+        unsigned long long* r = gres + 3 * (size_t)W.gid;
+        if (W.cnt) atomicAdd(&r[0], W.cnt);
+        if (W.hash) atomicAdd(&r[1], W.hash);
+        if (W.nonmax) atomicAdd(&r[2], W.nonmax);
+      }
+      W.cnt = W.hash = W.nonmax = 0;
       uint64_t te = globaltimer_ns();
       busy_ns += te - tb;
       last_done_ns = te - t_start;
       ++n_tasks;
       if (te - tb > max_task) {
         max_task = te - tb;
-        int nl = t.v[0] >= 0 ? g.row_off[t.v[0] + 1] - g.row_off[t.v[0]] : 0;
+        int nl = t.v[0] >= 0 ? W.gp->row_off[t.v[0] + 1] - W.gp->row_off[t.v[0]] : 0;
         max_info = ((unsigned long long)(unsigned)t.v[0] << 32) | (unsigned)nl;
       }
       if (lane == 0) {
@@ -1479,7 +1520,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     }
     int finished = 0;
     if (lane == 0) {
-      finished = (*(volatile int32_t*)&ctl->next_root >= nroots &&
+      finished = (*(volatile long long*)&ctl->next_root >= nroots &&
                   *(volatile unsigned long long*)&ctl->pending == 0ULL)
                      ? 1
                      : 0;
@@ -1500,9 +1541,6 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   }
   __syncwarp();
   if (lane == 0) {
-    if (W.cnt) atomicAdd(&ctl->count, W.cnt);
-    if (W.hash) atomicAdd(&ctl->hash, W.hash);
-    if (W.nonmax) atomicAdd(&ctl->non_maximal, W.nonmax);
     if (W.splits) atomicAdd(&ctl->tasks_split, W.splits);
     atomicAdd(&ctl->ns_setup, (unsigned long long)(busy_ns - W.ns_t1 - W.ns_t2));
     atomicAdd(&ctl->ns_tier1, (unsigned long long)W.ns_t1);

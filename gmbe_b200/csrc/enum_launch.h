@@ -11,13 +11,16 @@ constexpr int kEnumWarps = 16;                 // warps per block
 constexpr int kEnumThreads = kEnumWarps * 32;  // threads per block
 constexpr int kKMax = 4;                       // bitmap words of the tier-2 sub-problem
 
-__global__ void mbe_enum_kernel(const __grid_constant__ DevGraph g,
-                                const __grid_constant__ EnumParams p,
+// One persistent launch over p.n_graphs graphs: graphs[i] describes graph i,
+// root_prefix[i] counts the roots of graphs before i (root_prefix[n] = all),
+// gres[3i .. 3i+2] receives graph i's count, set hash and non-maximal count.
+__global__ void mbe_enum_kernel(const DevGraph* graphs, const long long* root_prefix,
+                                unsigned long long* gres, const __grid_constant__ EnumParams p,
                                 const __grid_constant__ ScratchLayout sl, EnumCtl* ctl,
                                 Task* q_tasks, unsigned long long* q_seq, SlotPool pool,
                                 int32_t* scratch, unsigned long long* exit_ns);
 
-constexpr int kSlotWordsHost = 16384;  // int32 words per sub-problem slot (64 KiB)
+constexpr int kSlotWordsHost = 32768;  // int32 words per sub-problem slot (128 KiB)
 
 // Per-warp scratch layout for the given capacities.
 ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS);

@@ -213,8 +213,11 @@ extern "C" int mbe_gen_batch_spec(uint64_t seed, mbe_gen_spec* out) {
   out->nV = std::max<int64_t>(2, (int64_t)std::llround(std::exp(lu) * std::exp(lr)));
   out->n_edges = (int64_t)std::llround(avg * (double)out->nU);
   out->gamma_u = out->gamma_v = 2.2;
-  out->max_deg_u = out->nV;
-  out->max_deg_v = out->nU;
+  // No degree cap is named for this distribution; Chung-Lu's own condition
+  // for edge probabilities to stay below 1 is w_max <= sqrt(total weight).
+  const int64_t cap = std::max<int64_t>(2, (int64_t)std::sqrt((double)out->n_edges));
+  out->max_deg_u = std::min<int64_t>(cap, out->nV);
+  out->max_deg_v = std::min<int64_t>(cap, out->nU);
   out->seed = seed;
   out->pair_p_max = 0.1;
   return MBE_OK;

@@ -15,8 +15,7 @@
 #include <cstring>
 #include <mutex>
 
-#include "enum_launch.h"
-#include "internal.h"
+#include "engine.h"
 
 namespace {
 
@@ -55,11 +54,24 @@ __global__ void noalloc_keys(uint64_t* ukey, int32_t nU, uint64_t* vkey, int32_t
   }
 }
 
-__global__ void noalloc_finish(const gmbe::EnumCtl* ctl, unsigned long long* out) {
+// Places the graph descriptor and the root prefix in the pool and zeroes the
+// per-graph results (a kernel, so no host copy is involved).
+__global__ void noalloc_init(const gmbe::DevGraph dg, gmbe::DevGraph* d_graph, long long* prefix,
+                             unsigned long long* gres) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    out[0] = ctl->count;
-    out[1] = ctl->hash;
-    out[2] = ctl->non_maximal;
+    *d_graph = dg;
+    prefix[0] = 0;
+    prefix[1] = dg.n_roots;
+    gres[0] = gres[1] = gres[2] = 0;
+  }
+}
+
+__global__ void noalloc_finish(const gmbe::EnumCtl* ctl, const unsigned long long* gres,
+                               unsigned long long* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    out[0] = gres[0];
+    out[1] = gres[1];
+    out[2] = gres[2];
     out[3] = (unsigned long long)(long long)ctl->status;
   }
 }
@@ -124,6 +136,9 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
     return o;
   };
   const size_t o_ctl = take(sizeof(EnumCtl));
+  const size_t o_graph = take(sizeof(DevGraph));
+  const size_t o_prefix = take(2 * sizeof(long long));
+  const size_t o_gres = take(3 * sizeof(unsigned long long));
   const size_t o_qt = take(sizeof(Task) * kNoAllocQueueCap);
   const size_t o_qs = take(sizeof(unsigned long long) * kNoAllocQueueCap);
   const size_t o_exit = take(2 * sizeof(unsigned long long) * kNoAllocMaxBlocks);
@@ -151,6 +166,9 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   const int warps = blocks * kEnumWarps;
 
   EnumCtl* ctl = reinterpret_cast<EnumCtl*>(pool + o_ctl);
+  DevGraph* d_graph = reinterpret_cast<DevGraph*>(pool + o_graph);
+  long long* d_prefix = reinterpret_cast<long long*>(pool + o_prefix);
+  unsigned long long* d_gres = reinterpret_cast<unsigned long long*>(pool + o_gres);
   Task* q_tasks = reinterpret_cast<Task*>(pool + o_qt);
   unsigned long long* q_seq = reinterpret_cast<unsigned long long*>(pool + o_qs);
   unsigned long long* exit_ns = reinterpret_cast<unsigned long long*>(pool + o_exit);
@@ -186,27 +204,27 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   dg.root_offset = 0;
   dg.root_stride = 1;
   dg.n_roots = nV;
-  int t2 = prm.bitmap_max_l == 0 ? 32 * kKMax : (prm.bitmap_max_l < 0 ? 1 : prm.bitmap_max_l);
-  if (t2 > 32 * kKMax) return set_error(MBE_ERR_INVALID, "bitmap_max_l > %d", 32 * kKMax);
+  mbe_params tune = prm;
+  tune.direct_max_c = 1 << 30;  // bitmap tier straight from set-up whenever |L| allows
+  int rc = apply_tuning(tune, &dg);
+  if (rc) return rc;
   EnumParams ep;
   memset(&ep, 0, sizeof(ep));
-  ep.bound_height = prm.bound_height;
-  ep.bound_size = prm.bound_size;
   ep.prune = prm.prune;
+  ep.n_graphs = 1;
   ep.queue_cap = kNoAllocQueueCap;
   ep.slot_spin_limit = 20000000;
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
   ep.record_exit = 0;
-  ep.tier2_max_l = t2;
-  ep.direct_max_c = 1 << 30;  // bitmap tier straight from set-up whenever |L| allows
   SlotPool none;
   none.slots = nullptr;
   none.bits = nullptr;
   none.nslot = 0;  // no sub-problem export out of the static pool
   ep.vertex_split = 1;
-  mbe_enum_kernel<<<blocks, kEnumThreads, 0, st>>>(dg, ep, sl, ctl, q_tasks, q_seq, none, scratch,
-                                                   exit_ns);
-  noalloc_finish<<<1, 32, 0, st>>>(ctl, d_out);
+  noalloc_init<<<1, 32, 0, st>>>(dg, d_graph, d_prefix, d_gres);
+  mbe_enum_kernel<<<blocks, kEnumThreads, 0, st>>>(d_graph, d_prefix, d_gres, ep, sl, ctl, q_tasks,
+                                                   q_seq, none, scratch, exit_ns);
+  noalloc_finish<<<1, 32, 0, st>>>(ctl, d_gres, d_out);
   if ((e = cudaGetLastError()) != cudaSuccess)
     return set_error(MBE_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
   return MBE_OK;

@@ -188,6 +188,44 @@ int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int32_t* d_col,
                                  int64_t nE, int64_t max_two_hop, const mbe_params* params,
                                  unsigned long long* d_out, void* stream);
 
+/* ---- batched enumeration ---------------------------------------------------
+ * No counterpart in the reference (it enumerates one graph per process,
+ * src/main.cu).  Many graphs in one device arena and one persistent launch,
+ * captured in a CUDA graph on the first run and replayed after that. */
+typedef struct mbe_batch mbe_batch;
+
+/* Builds a batch from n .adj-shaped host CSRs (graph i: row_offs[i] with
+ * nVs[i]+1 entries, cols[i] with nEs[i] entries; nUs may be NULL = max id+1).
+ * Each graph gets the same -t/-o treatment as mbe_graph_from_csr. */
+int mbe_batch_from_csr(int32_t n, const int32_t* const* row_offs, const int32_t* const* cols,
+                       const int32_t* nVs, const int32_t* nUs, const int64_t* nEs,
+                       const mbe_opts* opts, mbe_batch** out);
+int mbe_batch_size(const mbe_batch* b);
+
+/* Per-graph tuning (bound_height, bound_size, bitmap_max_l, direct_max_c of
+ * `p`) for graph `index` (-1 = all).  Results do not depend on it. */
+int mbe_batch_set_tuning(mbe_batch* b, int32_t index, const mbe_params* p);
+int mbe_batch_get_tuning(const mbe_batch* b, int32_t index, mbe_params* out);
+
+/* Enumerates every graph of the batch in one launch.  `params` supplies the
+ * launch-wide settings (pruning, split mode, blocks, queue, wait limit);
+ * per_graph (n entries, may be NULL) gets count / set_hash / non_maximal per
+ * graph in input order; total (may be NULL) gets the sums, the kernel time
+ * and the profile counters. */
+int mbe_batch_run(mbe_batch* b, const mbe_params* params, mbe_result* per_graph,
+                  mbe_result* total);
+
+/* Chooses per-graph tuning by size class: the graphs are split into
+ * n_classes quantiles of estimated work (sum of squared U degrees), and for
+ * each class a set of candidate tunings is timed on that class alone; the
+ * fastest is kept.  Every candidate must reproduce the same per-graph count
+ * and set hash, else MBE_ERR_CUDA.  chosen (n_classes entries, may be NULL)
+ * receives the candidate picked per class. */
+int mbe_batch_autotune(mbe_batch* b, const mbe_params* params, int32_t n_classes,
+                       int32_t* chosen);
+
+int mbe_batch_free(mbe_batch* b);
+
 /* ---- synthetic inputs ------------------------------------------------------
  * Seeded Chung-Lu bipartite generator (splitmix64 stream, Vose alias
  * sampling): expected degree of vertex i proportional to (i+1)^(-1/(gamma-1)),
@@ -218,7 +256,9 @@ int mbe_gen_chung_lu(const mbe_gen_spec* spec, int32_t** row_off, int32_t** col,
 
 /* The batched-mode size distribution: from `seed`, |U| log-uniform in
  * [50, 5000], |V|/|U| log-uniform in [0.5, 4], average U degree uniform in
- * [3, 30], exponent 2.2 on both sides, pair probability cap 0.1. */
+ * [3, 30], exponent 2.2 on both sides, expected-degree cap sqrt(edges)
+ * (Chung-Lu's condition for edge probabilities below 1), pair probability
+ * cap 0.1. */
 int mbe_gen_batch_spec(uint64_t seed, mbe_gen_spec* out);
 
 /* Write an .adj file (one line per V row, space-separated ascending U ids). */
