@@ -57,7 +57,8 @@ class Params(C.Structure):
                 ("bitmap_max_l", C.c_int32), ("wait_limit_ns", C.c_int64),
                 ("sm_timing", C.c_int32), ("root_begin", C.c_int32), ("root_end", C.c_int32),
                 ("shard_count", C.c_int32), ("shard_index", C.c_int32),
-                ("split_mode", C.c_int32), ("direct_max_c", C.c_int32)]
+                ("split_mode", C.c_int32), ("direct_max_c", C.c_int32),
+                ("root_split_size", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -69,7 +70,9 @@ class Result(C.Structure):
                 ("tier1_ms", C.c_double), ("tier2_ms", C.c_double), ("idle_ms", C.c_double),
                 ("max_task_ms", C.c_double), ("max_task_root", C.c_int32),
                 ("max_task_degree", C.c_int32), ("n_tasks", C.c_uint64),
-                ("n_subproblems", C.c_uint64)]
+                ("n_subproblems", C.c_uint64), ("max_task_tier1_ms", C.c_double),
+                ("max_task_tier2_ms", C.c_double), ("max_task_graph", C.c_int32),
+                ("reserved", C.c_int32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

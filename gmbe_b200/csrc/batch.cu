@@ -101,7 +101,8 @@ int upload_descriptors(mbe_batch* b, const std::vector<char>* active) {
 
 bool same_global(const mbe_params& a, const mbe_params& c) {
   return a.prune == c.prune && a.blocks == c.blocks && a.queue_capacity == c.queue_capacity &&
-         a.wait_limit_ns == c.wait_limit_ns && a.split_mode == c.split_mode;
+         a.wait_limit_ns == c.wait_limit_ns && a.split_mode == c.split_mode &&
+         a.root_split_size == c.root_split_size;
 }
 
 // Captures (or re-captures) the launch when the workspace or the global
@@ -348,6 +349,8 @@ int mbe_batch_run(mbe_batch* b, const mbe_params* params, mbe_result* per_graph,
     }
     total->kernel_ms = ms;
     fill_profile(*b->h_ctl, total);
+    if (total->max_task_graph >= 0 && total->max_task_graph < b->n)
+      total->max_task_graph = b->order[total->max_task_graph];  // input index
     total->enum_seconds = (now_ms() - t0) / 1e3;
   }
   return rc;

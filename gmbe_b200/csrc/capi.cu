@@ -277,6 +277,8 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
   ep.record_exit = prm.sm_timing ? 1 : 0;
   ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
+  // Heavy roots split into vertex tuples (sub-problem sharing mode only).
+  ep.root_split = prm.split_mode == 1 ? 0 : std::max(prm.root_split_size, 0);
   ep.n_graphs = spec.n_graphs;
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;
@@ -340,6 +342,9 @@ void fill_profile(const EnumCtl& ctl, mbe_result* out) {
   out->max_task_ms = ctl.max_task_ns / 1e6;
   out->max_task_root = (int32_t)(ctl.max_task_info >> 32);
   out->max_task_degree = (int32_t)(ctl.max_task_info & 0xffffffffu);
+  out->max_task_tier1_ms = (double)(ctl.max_task_split & 0xffffffffu) / 1e3;
+  out->max_task_tier2_ms = (double)(ctl.max_task_split >> 32) / 1e3;
+  out->max_task_graph = (int32_t)ctl.max_task_graph;
   out->n_tasks = ctl.n_tasks;
   out->n_subproblems = ctl.n_tier2;
 }

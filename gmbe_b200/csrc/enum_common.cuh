@@ -62,6 +62,8 @@ struct EnumCtl {
   unsigned long long ns_setup, ns_tier1, ns_tier2, ns_idle;
   unsigned long long max_task_ns;   // longest single task
   unsigned long long max_task_info; // (root << 32) | |L| of that task
+  unsigned long long max_task_split; // its counts-tier us | bitmap-tier us << 32
+  unsigned long long max_task_graph; // its graph
   unsigned long long n_tasks, n_tier2;
 };
 
@@ -96,7 +98,7 @@ struct EnumParams {
   int32_t record_exit;        // -p
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)
-  int32_t pad;
+  int32_t root_split;         // > 0: a root task with |P|*|L| above this splits into vertex tuples
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

@@ -153,23 +153,39 @@ __device__ void slot_free(Warp& W, int s) { atomicAnd(&W.slot_bits[s >> 5], ~(1u
 
 __device__ bool queue_push_one(Warp& W, const Task& t);
 
-// True when idle warps outnumber queued work (lane-uniform).
-__device__ bool export_wanted(Warp& W) {
+// Demand for exported work (lane-uniform): 0 none, 1 idle warps outnumber
+// queued work, 2 more than an eighth of all warps are idle as well.
+__device__ int export_demand(Warp& W) {
   int want = 0;
   if (lane_id() == 0) {
     EnumCtl* c = W.ctl;
     int idle = *(volatile int32_t*)&c->idle_warps;
     unsigned long long queued = *(volatile unsigned long long*)&c->q_tail -
                                 *(volatile unsigned long long*)&c->q_head;
-    want = idle > 0 && (unsigned long long)idle > queued;
+    if (idle > 0 && (unsigned long long)idle > queued) {
+      const int warps = (int)(gridDim.x * (blockDim.x >> 5));
+      want = idle > (warps >> 3) ? 2 : 1;
+    }
   }
-  return __shfl_sync(0xffffffffu, want, 0) != 0;
+  return __shfl_sync(0xffffffffu, want, 0);
 }
 
 // GMBE's split test on a child: (|P| > h or |L| > h) and |P| * |L| > s.
 __device__ __forceinline__ bool big_enough(const Warp& W, int nP, int nL) {
   return (nP > W.gp->bound_height || nL > W.gp->bound_height) &&
          (long long)nP * nL > (long long)W.gp->bound_size;
+}
+
+// Whether to hand a child (nP P-candidates, |L| = nL) to another warp.  A
+// child that passes GMBE's split test goes whenever warps wait for work.
+// When many warps wait, any child with a choice left goes too: the size test
+// misjudges dense graphs, where a few dozen candidates can hold millions of
+// bicliques, and an idle warp costs more than copying a small child.
+__device__ bool should_export(Warp& W, int nP, int nL) {
+  if (nP < 2 || nL < 2) return false;
+  const bool big = big_enough(W, nP, nL);
+  const int d = export_demand(W);
+  return d == 2 || (d == 1 && big);
 }
 
 // Enqueues a filled slot as a task; false if the ring is full.
@@ -198,7 +214,7 @@ __device__ void slot_header(int32_t* sp, int K, int nsub, int nq, const uint32_t
 template <int K>
 __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, int nchild,
                               int nbefore, const uint32_t* Ln, int kn, uint64_t sR, uint64_t nR) {
-  if (nchild > slot_cap(K) || !big_enough(W, nchild - nbefore, kn) || !export_wanted(W))
+  if (nchild > slot_cap(K) || !should_export(W, nchild - nbefore, kn))
     return false;
   const int lane = (int)lane_id();
   int slot = lane == 0 ? slot_alloc(W) : 0;
@@ -471,8 +487,14 @@ __device__ void tier2(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t n
   tier2_dispatch(W, src, words_k(n));
 }
 
-// Runs an exported sub-problem and releases its slot.
+// Runs an exported sub-problem and releases its slot.  The slot was written
+// by another warp, possibly on another SM, and may have been read here
+// before under an older owner: every lane fences before its first read.
+// The run writes bounds into the slot's level-0 records, so every lane
+// fences again before the slot is freed; without that a store still in
+// flight could land on the records of the slot's next owner.
 __device__ void tier2_from_slot(Warp& W, int slot) {
+  __threadfence();
   int32_t* sp = W.slots + (size_t)slot * kSlotWords;
   T2Src src;
   const int K = sp[0];
@@ -487,6 +509,7 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   src.rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
   src.subkey = slot_subkey(sp, K, src.nsub);
   tier2_dispatch(W, src, K);
+  __threadfence();
   __syncwarp();
   if (lane_id() == 0) slot_free(W, slot);
   __syncwarp();
@@ -746,7 +769,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
     // big enough by GMBE's split test, else this warp's scratch.
     const int K = words_k(n), RS = K + 1;
     int slot = -1;
-    if (ncand <= slot_cap(K) && big_enough(W, ncand - nqc, n) && export_wanted(W)) {
+    if (ncand <= slot_cap(K) && should_export(W, ncand - nqc, n)) {
       slot = lane == 0 ? slot_alloc(W) : 0;
       slot = __shfl_sync(kFull, slot, 0);
     }
@@ -1304,10 +1327,17 @@ __device__ void run_task(Warp& W, const Task& t) {
   }
   bool done = nL <= 1 || np == 0;
   // ---- split (src/IterFinderGpu.cu:835-858) ----
-  if (!done && k < 4 && W.p.vertex_split) {
+  // A heavy root splits the same way in the sub-problem sharing mode: its
+  // first level alone would otherwise run on one warp for the whole launch.
+  if (!done && k < 4) {
     long long rest = np;
-    if ((rest > W.gp->bound_height || nL > W.gp->bound_height) &&
-        rest * (long long)nL > (long long)W.gp->bound_size) {
+    bool split;
+    if (W.p.vertex_split)
+      split = (rest > W.gp->bound_height || nL > W.gp->bound_height) &&
+              rest * (long long)nL > (long long)W.gp->bound_size;
+    else
+      split = k == 1 && W.p.root_split > 0 && rest * (long long)nL > (long long)W.p.root_split;
+    if (split) {
       if (queue_push_children(W, t, k, nq, nC)) {
         W.splits += 1;
         done = true;
@@ -1452,7 +1482,8 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   W.gid = 0;
   W.cnt = W.hash = W.nonmax = W.splits = 0;
   W.ns_t1 = W.ns_t2 = W.n_t2 = 0;
-  uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0;
+  uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0, max_split = 0;
+  int32_t max_gid = 0;
   const long long nroots = root_prefix[p.n_graphs];
   uint64_t idle_since = 0;
   uint64_t busy_ns = 0, last_done_ns = 0, idle_last = 0;
@@ -1486,6 +1517,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
       t.graph = __shfl_sync(kFull, t.graph, 0);
       if (idle_since != 0 && lane == 0) atomicSub(&ctl->idle_warps, 1);
       uint64_t tb = globaltimer_ns();
+      const unsigned long long t1_before = W.ns_t1, t2_before = W.ns_t2;
       if (t.v[0] >= 0) {
         W.gid = t.graph;
         W.gp = graphs + t.graph;
@@ -1510,6 +1542,8 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
         max_task = te - tb;
         int nl = t.v[0] >= 0 ? W.gp->row_off[t.v[0] + 1] - W.gp->row_off[t.v[0]] : 0;
         max_info = ((unsigned long long)(unsigned)t.v[0] << 32) | (unsigned)nl;
+        max_split = (W.ns_t1 - t1_before) / 1000 | ((W.ns_t2 - t2_before) / 1000 << 32);
+        max_gid = W.gid;
       }
       if (lane == 0) {
         __threadfence();
@@ -1549,7 +1583,12 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
     atomicAdd(&ctl->n_tasks, (unsigned long long)n_tasks);
     atomicAdd(&ctl->n_tier2, (unsigned long long)W.n_t2);
     unsigned long long old = atomicMax(&ctl->max_task_ns, (unsigned long long)max_task);
-    if (old < max_task) atomicExch(&ctl->max_task_info, (unsigned long long)max_info);
+    if (old < max_task) {
+      atomicExch(&ctl->max_task_info, (unsigned long long)max_info);
+      // (counts-tier us) | (bitmap-tier us << 32), and the task's graph
+      atomicExch(&ctl->max_task_split, (unsigned long long)max_split);
+      atomicExch(&ctl->max_task_graph, (unsigned long long)max_gid);
+    }
   }
   if (p.record_exit) {
     // Per block: when its last task finished, and its warps' summed busy time.

@@ -119,6 +119,11 @@ extern "C" int mbe_gen_chung_lu(const mbe_gen_spec* spec, int32_t** row_off_out,
     return set_error(MBE_ERR_INVALID, "planted blocks do not fit");
   SplitMix64 rng(s.seed);
   int64_t target = std::min<int64_t>(s.n_edges, s.nU * s.nV);
+  // Under a pair-probability cap the graph's density cannot exceed the cap:
+  // an edge target above cap * |U| * |V| would be reached only by drawing
+  // until nearly every pair is taken (a near-complete block).
+  if (s.pair_p_max > 0 && s.pair_p_max < 1)
+    target = std::min<int64_t>(target, std::max<int64_t>(1, (int64_t)(s.pair_p_max * (double)s.nU * (double)s.nV)));
   std::vector<double> wu = power_law_weights(s.nU, s.gamma_u, s.max_deg_u, (double)target);
   std::vector<double> wv = power_law_weights(s.nV, s.gamma_v, s.max_deg_v, (double)target);
   Alias au(wu), av(wv);

@@ -94,6 +94,10 @@ typedef struct mbe_params {
   int32_t direct_max_c;    /* a task with |L| <= bitmap_max_l goes straight to the bitmap  */
                            /*   tier only while |C| <= this (0 = 4096); larger candidate   */
                            /*   sets go through the counts tier's sparse pushes            */
+  int32_t root_split_size; /* split_mode 0: a root task (one vertex) with |P|*|L| above    */
+                           /*   this is split into GMBE's vertex-tuple child tasks, so a   */
+                           /*   heavy root's first level runs on many warps; deeper levels */
+                           /*   still share out sub-problems.  <= 0 = never (default)      */
 } mbe_params;
 
 typedef struct mbe_result {
@@ -113,6 +117,10 @@ typedef struct mbe_result {
   double setup_ms, tier1_ms, tier2_ms, idle_ms, max_task_ms;
   int32_t max_task_root, max_task_degree;
   uint64_t n_tasks, n_subproblems;
+  /* The longest task's time in the counts and bitmap tiers, and its graph
+   * (the launch's graph index: descriptor order in a batch). */
+  double max_task_tier1_ms, max_task_tier2_ms;
+  int32_t max_task_graph, reserved;
 } mbe_result;
 
 /* Default parameters: bound_height 20, bound_size 1500, prune 1. */
@@ -235,7 +243,8 @@ int mbe_batch_free(mbe_batch* b);
  * (u,v) pair at pair_p_max: a draw is kept with probability
  * min(1, -ln(1-pair_p_max) / (w_u w_v / sum w)).  Without the cap, hubs whose
  * weight product exceeds the edge count form a near-complete block whose few
- * missing edges give exponentially many maximal bicliques.
+ * missing edges give exponentially many maximal bicliques.  With the cap the
+ * edge target is also clamped to pair_p_max * nU * nV.
  * Optional planted blocks: n_blocks disjoint (block_u x block_v) vertex sets,
  * each pair an edge with probability block_p.  Not part of the reference
  * (its inputs are downloaded datasets, preprocess/prepare_dataset.sh). */

@@ -216,3 +216,29 @@ def test_csr_validation_runs_before_any_device_call(gm):
 def test_params_defaults(gm):
     p = gm.default_params()
     assert (p.bound_height, p.bound_size, p.prune) == (20, 1500, 1)
+
+
+def test_ctypes_mirrors_match_the_c_header(gm, tmp_path):
+    # The Python binding mirrors the C structs field by field; a field added
+    # on one side only would make the library write past the caller's struct.
+    # gcc compiles a probe against include/mbe.h that prints each struct's
+    # size and every field's offset.
+    mirrors = {"mbe_opts": gm.Opts, "mbe_graph_info": gm.GraphInfo, "mbe_params": gm.Params,
+               "mbe_result": gm.Result, "mbe_gen_spec": gm.GenSpec}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mbe.h"', 'int main(void) {']
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-I", inc, "-o", str(exe), str(src)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                 text=True).stdout.splitlines())
+    for cname, py in mirrors.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"

@@ -152,3 +152,51 @@ def test_idle_wait_limit_reports_timeout_then_recovers(gm):
         assert ei.value.name == "MBE_ERR_TIMEOUT"
         r = G.enumerate()
         assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+@pytest.mark.parametrize("shape", [(24, 36, 0.85), (26, 40, 0.88)])
+def test_dense_small_graph_is_shared_out(gm, shape):
+    # A few dozen vertices at high density hold 10^5 - 10^6 bicliques under a
+    # handful of roots: exact results, and the work must be spread over warps
+    # (the split test by |P| * |L| alone would keep each root in one warp).
+    nV, nU, p = shape
+    ro, co, nU = random_bipartite(nV, nU, p, 1)
+    want = oracle.gmbe(ro, co, nU)
+    with gm.Graph.from_csr(ro, co, nU) as G:
+        r = G.enumerate(sm_timing=1)
+    assert (r.count, r.set_hash) == (want.count, want.set_hash)
+    assert r.n_subproblems > 4 * nV
+
+
+@pytest.mark.parametrize("root_split", [0, 1, 64, 1 << 20])
+def test_root_split_threshold_does_not_change_result(gm, root_split):
+    # Heavy roots split into vertex-tuple child tasks (GMBE's own split) while
+    # deeper levels share out sub-problems: any threshold gives the same set.
+    for ro, co, nU in (planted(300, 200, blocks=6, seed=3, bsize=14), hub_graph(1)):
+        want = oracle.gmbe(ro, co, nU)
+        r = run(gm, ro, co, nU, root_split_size=root_split)
+        assert r.status == 0
+        assert (r.count, r.set_hash) == (want.count, want.set_hash)
+        if root_split == 1:
+            assert r.tasks_split > 0
+
+
+def test_slot_reuse_across_graphs_is_exact(gm):
+    # Small dense graphs keep most warps idle, so nearly every child is shared
+    # out and the sub-problem slots are freed and reused constantly, by warps
+    # on different SMs and across launches on different graphs.  Alternating
+    # graphs back to back, every run must still be exact.
+    shapes = [(24, 36, 0.85, 1), (26, 40, 0.8, 2), (30, 30, 0.75, 3), (20, 44, 0.85, 4)]
+    graphs = []
+    for nV, nU, p, seed in shapes:
+        ro, co, nU = random_bipartite(nV, nU, p, seed)
+        want = oracle.gmbe(ro, co, nU)
+        graphs.append((gm.Graph.from_csr(ro, co, nU), (want.count, want.set_hash)))
+    try:
+        for rep in range(25):
+            for i, (G, want) in enumerate(graphs):
+                r = G.enumerate()
+                assert (r.count, r.set_hash) == want, f"graph {i} repeat {rep}"
+    finally:
+        for G, _ in graphs:
+            G.free()
