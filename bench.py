@@ -278,7 +278,7 @@ def main():
     e2e_steps = max(1, min(args.steps, 3))
     # CSR, its transpose and the per-vertex hash keys are uploaded per call.
     h2d = 4 * ((g.nV + 1) + (g.nU + 1) + 2 * g.nE) + 8 * (g.nV + g.nU)
-    d2h = 152  # the result block read back per call
+    d2h = 176 + 24  # per call: the launch's control block and the graph's result triple
     e2e_s = []
     G.free()
     for _ in range(e2e_steps):

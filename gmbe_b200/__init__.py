@@ -58,7 +58,7 @@ class Params(C.Structure):
                 ("sm_timing", C.c_int32), ("root_begin", C.c_int32), ("root_end", C.c_int32),
                 ("shard_count", C.c_int32), ("shard_index", C.c_int32),
                 ("split_mode", C.c_int32), ("direct_max_c", C.c_int32),
-                ("root_split_size", C.c_int32)]
+                ("root_split_size", C.c_int32), ("share_min_work", C.c_int32)]
 
 
 class Result(C.Structure):

@@ -279,6 +279,7 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
   // Heavy roots split into vertex tuples (sub-problem sharing mode only).
   ep.root_split = prm.split_mode == 1 ? 0 : std::max(prm.root_split_size, 0);
+  ep.share_min_work = prm.share_min_work > 0 ? prm.share_min_work : kShareMinWorkDefault;
   ep.n_graphs = spec.n_graphs;
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;

@@ -99,6 +99,8 @@ struct EnumParams {
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)
   int32_t root_split;         // > 0: a root task with |P|*|L| above this splits into vertex tuples
+  int32_t share_min_work;     // |P|*|L| of a child shared out while many warps wait
+  int32_t pad;
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

@@ -178,14 +178,15 @@ __device__ __forceinline__ bool big_enough(const Warp& W, int nP, int nL) {
 
 // Whether to hand a child (nP P-candidates, |L| = nL) to another warp.  A
 // child that passes GMBE's split test goes whenever warps wait for work.
-// When many warps wait, any child with a choice left goes too: the size test
-// misjudges dense graphs, where a few dozen candidates can hold millions of
-// bicliques, and an idle warp costs more than copying a small child.
+// When many warps wait, smaller children go too: the size test misjudges
+// dense graphs, where a few dozen candidates can hold millions of
+// bicliques.  The floor (share_min_work) keeps the tiniest children, whose
+// copy would cost the exporting warp more than running them, at home.
 __device__ bool should_export(Warp& W, int nP, int nL) {
   if (nP < 2 || nL < 2) return false;
   const bool big = big_enough(W, nP, nL);
   const int d = export_demand(W);
-  return d == 2 || (d == 1 && big);
+  return (d == 2 && (big || (long long)nP * nL >= W.p.share_min_work)) || (d == 1 && big);
 }
 
 // Enqueues a filled slot as a task; false if the ring is full.

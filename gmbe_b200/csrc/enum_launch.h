@@ -21,6 +21,8 @@ __global__ void mbe_enum_kernel(const DevGraph* graphs, const long long* root_pr
                                 int32_t* scratch, unsigned long long* exit_ns);
 
 constexpr int kSlotWordsHost = 32768;  // int32 words per sub-problem slot (128 KiB)
+// |P|*|L| from which a child is shared out while many warps wait for work.
+constexpr int32_t kShareMinWorkDefault = 64;
 
 // Per-warp scratch layout for the given capacities.
 ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS);

@@ -98,6 +98,9 @@ typedef struct mbe_params {
                            /*   this is split into GMBE's vertex-tuple child tasks, so a   */
                            /*   heavy root's first level runs on many warps; deeper levels */
                            /*   still share out sub-problems.  <= 0 = never (default)      */
+  int32_t share_min_work;  /* split_mode 0: while over an eighth of the warps wait for    */
+                           /*   work, any child with |P|*|L| >= this is shared out, beyond */
+                           /*   the split test's children (0 = default 64)                 */
 } mbe_params;
 
 typedef struct mbe_result {
