@@ -86,6 +86,22 @@ class GenSpec(C.Structure):
                 ("reserved", C.c_int32), ("block_p", C.c_double), ("pair_p_max", C.c_double)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_graphs", C.c_int32), ("arena_bytes", C.c_int64),
+                ("max_v", C.c_int32), ("max_degree", C.c_int32), ("max_two_hop", C.c_int32),
+                ("reserved", C.c_int32), ("idle_exit_ns", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("rejected", C.c_uint64), ("cancelled", C.c_uint64), ("launches", C.c_uint64),
+                ("arena_resets", C.c_uint64), ("resident", C.c_int64), ("waiting", C.c_int64),
+                ("arena_used", C.c_int64), ("arena_bytes", C.c_int64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _P32 = C.POINTER(C.c_int32)
 _sig = {
     "mbe_params_default": (None, [C.POINTER(Params)]),
@@ -114,6 +130,16 @@ _sig = {
                                 C.POINTER(Result)]),
     "mbe_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(Params), C.c_int32, _P32]),
     "mbe_batch_free": (C.c_int, [C.c_void_p]),
+    "mbe_server_config_default": (None, [C.POINTER(ServerConfig)]),
+    "mbe_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(Params),
+                                    C.POINTER(C.c_void_p)]),
+    "mbe_server_submit": (C.c_int, [C.c_void_p, _P32, _P32, C.c_int32, C.c_int32, C.c_int64,
+                                    C.POINTER(Opts), C.POINTER(C.c_uint64)]),
+    "mbe_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Result)]),
+    "mbe_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int64, C.POINTER(Result)]),
+    "mbe_server_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "mbe_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "mbe_server_destroy": (C.c_int, [C.c_void_p]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(_lib, _name)
@@ -261,6 +287,75 @@ class Batch:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching server on one GPU (mbe_server_* in include/mbe.h):
+    graphs submitted at any time share one persistent launch."""
+
+    def __init__(self, device=0, max_graphs=0, arena_bytes=0, max_v=0, max_degree=0,
+                 max_two_hop=0, idle_exit_ns=0, **params):
+        self._h = C.c_void_p()
+        cfg = ServerConfig()
+        _lib.mbe_server_config_default(C.byref(cfg))
+        cfg.device = device
+        for k, v in dict(max_graphs=max_graphs, arena_bytes=arena_bytes, max_v=max_v,
+                         max_degree=max_degree, max_two_hop=max_two_hop,
+                         idle_exit_ns=idle_exit_ns).items():
+            if v:
+                setattr(cfg, k, v)
+        p = default_params(**params)
+        h = C.c_void_p()
+        _check(_lib.mbe_server_create(C.byref(cfg), C.byref(p), C.byref(h)))
+        self._h = h
+
+    def submit(self, row_off, col, nU=0, uvtrans=1, order=1, fast_mode=1) -> int:
+        ro, co = _i32(row_off), _i32(col)
+        rid = C.c_uint64()
+        opts = make_opts(uvtrans, order, fast_mode)
+        _check(_lib.mbe_server_submit(self._h, _ptr(ro), _ptr(co), len(ro) - 1, int(nU),
+                                      len(co), C.byref(opts), C.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int):
+        """The finished request's Result, or None while it runs."""
+        r = Result()
+        rc = _lib.mbe_server_poll(self._h, rid, C.byref(r))
+        if rc == -12:  # MBE_ERR_AGAIN
+            return None
+        _check(rc)
+        return r
+
+    def wait(self, rid: int, timeout: float | None = None) -> Result:
+        r = Result()
+        ns = -1 if timeout is None else int(timeout * 1e9)
+        _check(_lib.mbe_server_wait(self._h, rid, ns, C.byref(r)))
+        return r
+
+    def cancel(self, rid: int):
+        _check(_lib.mbe_server_cancel(self._h, rid))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(_lib.mbe_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.mbe_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 

@@ -90,6 +90,45 @@ struct SlotPool {
   int32_t nslot;   // multiple of 32; 0 disables export
 };
 
+// Serving.  Every resident graph is one block of the device arena, aligned to
+// 1 << kServeBlockShift bytes and named by its block index: this header, then
+// its CSRs and hash keys (the descriptor's pointers point inside the block).
+// The host writes the whole block before it publishes the graph; the kernel
+// then updates only the counters.  Blocks are bump-allocated and the arena is
+// reset only between launches, so no address is rewritten while a launch may
+// hold it in a cache.
+constexpr int kServeBlockShift = 12;
+struct ServeGraph {
+  DevGraph g;
+  unsigned long long next_root;  // roots claimed (runs past n_roots once exhausted)
+  unsigned long long pending;    // roots not yet finished + queued or running children
+  unsigned long long res[3];     // count, set hash, non-maximal
+  unsigned long long request;    // the host's request id
+};
+
+// Completion record, in host-mapped memory; seq = position + 1 once written.
+struct ServeDone {
+  unsigned long long request, count, hash, non_maximal, seq;
+  unsigned long long pad[3];
+};
+
+// Serving state that outlives a launch (device memory).
+struct ServeCtl {
+  unsigned long long arr_tail;  // graphs published (written by the host)
+  unsigned long long arr_head;  // first published graph that may have roots left
+  unsigned long long done_pos;  // completion records handed out
+  int32_t stop;                 // written by the host: leave at once
+  int32_t pad;
+};
+
+struct ServeLink {
+  ServeCtl* sctl;
+  const uint32_t* arr_blk;  // block index of published graph k at k % arr_cap
+  ServeDone* done;          // completion ring (host-mapped)
+  int32_t arr_cap, done_cap;
+  int64_t idle_exit_ns;     // a launch ends after this long with nothing to do
+};
+
 struct EnumParams {
   int32_t prune;
   int32_t queue_cap;
@@ -100,7 +139,8 @@ struct EnumParams {
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)
   int32_t root_split;         // > 0: a root task with |P|*|L| above this splits into vertex tuples
   int32_t share_min_work;     // |P|*|L| of a child shared out while many warps wait
-  int32_t pad;
+  int32_t server;             // 1: graphs arrive while the launch runs (ServeLink)
+  ServeLink serve;
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

@@ -96,6 +96,24 @@ struct Warp {
   __device__ uint64_t* A64(int64_t off) const { return reinterpret_cast<uint64_t*>(base + off); }
 };
 
+// Serving block of graph `gid` (a block index into the arena, which the
+// launch receives in place of the descriptor array).
+__device__ __forceinline__ ServeGraph* serve_graph(const Warp& W, int32_t gid) {
+  char* arena = const_cast<char*>(reinterpret_cast<const char*>(W.graphs));
+  return reinterpret_cast<ServeGraph*>(arena + ((size_t)(uint32_t)gid << kServeBlockShift));
+}
+
+// Descriptor of graph `gid` of this launch.
+__device__ __forceinline__ const DevGraph* graph_at(const Warp& W, int32_t gid) {
+  return W.p.server ? &serve_graph(W, gid)->g : W.graphs + gid;
+}
+
+// Children of the current graph about to be queued (serving: a graph
+// completes when its roots and every queued child have finished).
+__device__ __forceinline__ void graph_spawned(const Warp& W, unsigned long long n) {
+  if (W.p.server) atomicAdd(&serve_graph(W, W.gid)->pending, n);
+}
+
 // ---------------------------------------------------------------------------
 // Bitmap sub-problems.
 //
@@ -502,7 +520,7 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   src.nsub = sp[1];
   src.nq = sp[2];
   W.gid = sp[3];
-  W.gp = W.graphs + W.gid;
+  W.gp = graph_at(W, W.gid);
   for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)sp[4 + w];
   src.sR0 = *reinterpret_cast<const uint64_t*>(sp + 8);
   src.nR0 = (uint32_t)sp[10];
@@ -1025,6 +1043,7 @@ __device__ bool queue_push_children(Warp& W, const Task& t, int k, int nq, int n
       atomicAdd(&ctl->q_used, (unsigned long long)(-(long long)n));
     } else {
       atomicAdd(&ctl->pending, n);
+      graph_spawned(W, n);
       pos = atomicAdd(&ctl->q_tail, n);
       ok = 1;
     }
@@ -1071,6 +1090,7 @@ __device__ bool queue_push_one(Warp& W, const Task& t) {
       atomicAdd(&ctl->q_used, (unsigned long long)-1LL);
     } else {
       atomicAdd(&ctl->pending, 1ULL);
+      graph_spawned(W, 1ULL);
       unsigned long long gp = atomicAdd(&ctl->q_tail, 1ULL);
       unsigned long long slot = gp % (unsigned long long)cap;
       volatile unsigned long long* st = W.q_seq + slot;
@@ -1461,6 +1481,59 @@ __device__ __forceinline__ int graph_of_position(const long long* prefix, int n,
   return lo;
 }
 
+// Serving: claims a root of the oldest published graph that has roots left
+// (lane 0).  Graphs are drained in publication order; a warp that finds the
+// head graph exhausted moves the head on.  As for a static launch, the
+// launch-wide pending count is raised before a claim but only while some
+// published graph may have roots left: idle warps polling an empty arrival
+// ring must leave it at zero, or the launch could never see itself quiet.
+// A warp that saw the head below the tail just before another moved it past
+// its graph claims nothing (that graph was exhausted), so the quiet test
+// (pending == 0, head >= tail) loses no root.
+__device__ bool serve_claim_root(Warp& W, Task* t) {
+  const ServeLink& L = W.p.serve;
+  volatile ServeCtl* sc = L.sctl;
+  if (sc->arr_head >= sc->arr_tail) return false;
+  atomicAdd(&W.ctl->pending, 1ULL);
+  for (int tries = 0; tries < 64; ++tries) {
+    const unsigned long long h = sc->arr_head;
+    if (h >= sc->arr_tail) break;
+    const uint32_t blk = *(volatile const uint32_t*)&L.arr_blk[h % (unsigned long long)L.arr_cap];
+    ServeGraph* sg = serve_graph(W, (int32_t)blk);
+    const unsigned long long r = atomicAdd(&sg->next_root, 1ULL);
+    const DevGraph& g = sg->g;
+    if (r < (unsigned long long)g.n_roots) {
+      t->v[0] = g.root_end - 1 - (g.root_offset + (int)r * g.root_stride);
+      t->v[1] = t->v[2] = t->v[3] = -1;
+      t->graph = (int32_t)blk;
+      return true;
+    }
+    atomicCAS((unsigned long long*)&L.sctl->arr_head, h, h + 1);
+  }
+  atomicAdd(&W.ctl->pending, (unsigned long long)-1LL);
+  return false;
+}
+
+// Serving: one task of graph `gid` finished (lane 0, after its results were
+// added).  The task that brings the graph's pending count to zero writes the
+// graph's completion record for the host.
+__device__ void serve_task_done(Warp& W, int32_t gid) {
+  const ServeLink& L = W.p.serve;
+  ServeGraph* sg = serve_graph(W, gid);
+  if (atomicAdd(&sg->pending, (unsigned long long)-1LL) != 1ULL) return;
+  __threadfence();
+  volatile ServeGraph* vs = sg;
+  const unsigned long long c = vs->res[0], h = vs->res[1], nm = vs->res[2], req = vs->request;
+  const unsigned long long pos = atomicAdd(&L.sctl->done_pos, 1ULL);
+  volatile ServeDone* d = L.done + (pos % (unsigned long long)L.done_cap);
+  d->request = req;
+  d->count = c;
+  d->hash = h;
+  d->non_maximal = nm;
+  __threadfence_system();
+  d->seq = pos + 1;
+}
+
 __global__ void __launch_bounds__(kEnumThreads, 1)
     mbe_enum_kernel(const DevGraph* graphs, const long long* root_prefix,
                     unsigned long long* gres, const __grid_constant__ EnumParams p,
@@ -1485,17 +1558,23 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   W.ns_t1 = W.ns_t2 = W.n_t2 = 0;
   uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0, max_split = 0;
   int32_t max_gid = 0;
-  const long long nroots = root_prefix[p.n_graphs];
+  const long long nroots = p.server ? 0 : root_prefix[p.n_graphs];
   uint64_t idle_since = 0;
   uint64_t busy_ns = 0, last_done_ns = 0, idle_last = 0;
   while (true) {
-    int ab = lane == 0 ? *(volatile int32_t*)&ctl->abort : 0;
+    int ab = 0;
+    if (lane == 0) {
+      ab = *(volatile int32_t*)&ctl->abort;
+      if (p.server) ab |= *(volatile int32_t*)&p.serve.sctl->stop;  // server shutting down
+    }
     if (__shfl_sync(kFull, ab, 0)) break;
     Task t;
     int have = 0;
     if (lane == 0) {
       have = queue_pop(W, &t) ? 1 : 0;
-      if (!have && *(volatile long long*)&ctl->next_root < nroots) {
+      if (!have && p.server) {
+        have = serve_claim_root(W, &t) ? 1 : 0;
+      } else if (!have && *(volatile long long*)&ctl->next_root < nroots) {
         atomicAdd(&ctl->pending, 1ULL);
         long long r = (long long)atomicAdd((unsigned long long*)&ctl->next_root, 1ULL);
         if (r < nroots) {
@@ -1521,7 +1600,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
       const unsigned long long t1_before = W.ns_t1, t2_before = W.ns_t2;
       if (t.v[0] >= 0) {
         W.gid = t.graph;
-        W.gp = graphs + t.graph;
+        W.gp = graph_at(W, t.graph);
         run_task(W, t);
       } else {
         tier2_from_slot(W, -2 - t.v[0]);  // an exported bitmap sub-problem (sets the graph)
@@ -1529,7 +1608,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
       __syncwarp();
       // Results go to the task's graph.
       if (lane == 0) {
-        unsigned long long* r = gres + 3 * (size_t)W.gid;
+        unsigned long long* r = p.server ? serve_graph(W, W.gid)->res : gres + 3 * (size_t)W.gid;
         if (W.cnt) atomicAdd(&r[0], W.cnt);
         if (W.hash) atomicAdd(&r[1], W.hash);
         if (W.nonmax) atomicAdd(&r[2], W.nonmax);
@@ -1548,26 +1627,40 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
       }
       if (lane == 0) {
         __threadfence();
+        if (p.server) serve_task_done(W, W.gid);
         atomicAdd(&ctl->pending, (unsigned long long)-1LL);
       }
       idle_since = 0;
       continue;
     }
+    // 1: leave now; 2 (serving): nothing in flight and no published roots left.
     int finished = 0;
     if (lane == 0) {
-      finished = (*(volatile long long*)&ctl->next_root >= nroots &&
-                  *(volatile unsigned long long*)&ctl->pending == 0ULL)
-                     ? 1
-                     : 0;
+      if (p.server) {
+        volatile ServeCtl* sc = p.serve.sctl;
+        if (sc->stop) finished = 1;
+        else if (*(volatile unsigned long long*)&ctl->pending == 0ULL && sc->arr_head >= sc->arr_tail)
+          finished = 2;
+      } else {
+        finished = (*(volatile long long*)&ctl->next_root >= nroots &&
+                    *(volatile unsigned long long*)&ctl->pending == 0ULL)
+                       ? 1
+                       : 0;
+      }
     }
     finished = __shfl_sync(kFull, finished, 0);
-    if (finished) break;
+    if (finished == 1) break;
     uint64_t now = globaltimer_ns();
     if (idle_since != 0) ns_idle += now - idle_last;
     idle_last = now;
     if (idle_since == 0) {
       idle_since = now;
       if (lane == 0) atomicAdd(&ctl->idle_warps, 1);
+    } else if (p.server && finished == 2 && now - idle_since > (uint64_t)p.serve.idle_exit_ns) {
+      // A serving launch ends once it has had nothing to do for a while; the
+      // host launches again when graphs arrive.
+      if (lane == 0) atomicSub(&ctl->idle_warps, 1);
+      break;
     } else if (now - idle_since > (uint64_t)p.idle_ns_limit) {
       if (lane == 0) set_status(ctl, kStTimeout, now - idle_since);
       break;

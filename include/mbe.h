@@ -237,6 +237,72 @@ int mbe_batch_autotune(mbe_batch* b, const mbe_params* params, int32_t n_classes
 
 int mbe_batch_free(mbe_batch* b);
 
+/* ---- serving ---------------------------------------------------------------
+ * No counterpart in the reference.  A server keeps graphs and enumeration
+ * state resident on one GPU and feeds them to one persistent launch while it
+ * runs (continuous batching): a request submitted while others are on the
+ * GPU is admitted as soon as arena memory and a graph slot are free, and its
+ * roots are then claimed by the same warps that work on the others.  A launch
+ * ends after idle_exit_ns with nothing to do; the server starts another when
+ * work arrives.  Per request the count, set hash and non-maximal count are
+ * exactly those of mbe_enumerate on the same CSR and options. */
+typedef struct mbe_server mbe_server;
+
+typedef struct mbe_server_config {
+  int32_t device;
+  int32_t max_graphs;   /* graphs admitted and not yet finished (0 = 4096) */
+  int64_t arena_bytes;  /* device memory for resident graphs (0 = 1 GiB) */
+  /* Per-warp capacities, fixed for the server's life.  A request whose
+   * internal V side, largest root degree or largest two-hop multiset of a
+   * root exceeds them can never run: mbe_server_submit rejects it with
+   * MBE_ERR_ADMISSION.  0 = 32768 / 4096 / 65536. */
+  int32_t max_v;
+  int32_t max_degree;
+  int32_t max_two_hop;
+  int32_t reserved;
+  int64_t idle_exit_ns; /* a launch ends after this long without work (0 = 200 us) */
+} mbe_server_config;
+
+typedef struct mbe_server_stats {
+  uint64_t submitted, admitted, completed, rejected, cancelled;
+  uint64_t launches;      /* persistent launches so far */
+  uint64_t arena_resets;  /* times the arena was rewound (nothing resident, no launch) */
+  int64_t resident;       /* admitted, not yet finished */
+  int64_t waiting;        /* submitted, not yet admitted */
+  int64_t arena_used, arena_bytes;
+} mbe_server_stats;
+
+void mbe_server_config_default(mbe_server_config* c);
+
+/* `params` (may be NULL = defaults) applies to every request. */
+int mbe_server_create(const mbe_server_config* cfg, const mbe_params* params, mbe_server** out);
+
+/* Copies and prepares one .adj-shaped CSR (the -t/-o of `opts`, as in
+ * mbe_graph_from_csr) and queues it; returns at once with its id.  Admission
+ * (arena space and a graph slot) is first come, first served.  Errors:
+ * MBE_ERR_FORMAT / MBE_ERR_INVALID for bad input, MBE_ERR_ADMISSION if the
+ * graph exceeds the server's capacities or arena. */
+int mbe_server_submit(mbe_server* s, const int32_t* row_off, const int32_t* col, int32_t nV,
+                      int32_t nU, int64_t nE, const mbe_opts* opts, uint64_t* request_id);
+
+/* Result of a finished request (then forgotten): MBE_OK with count, set_hash,
+ * non_maximal and enum_seconds = time from submit to result; MBE_ERR_AGAIN
+ * if not finished; MBE_ERR_NOT_FOUND for an unknown id; MBE_ERR_CANCELLED for
+ * a cancelled one; a launch failure's code for a request it took down. */
+int mbe_server_poll(mbe_server* s, uint64_t request_id, mbe_result* out);
+
+/* As mbe_server_poll, waiting up to timeout_ns (< 0 = no limit). */
+int mbe_server_wait(mbe_server* s, uint64_t request_id, int64_t timeout_ns, mbe_result* out);
+
+/* Withdraws a request that is not yet admitted (MBE_OK); one already on the
+ * GPU or finished cannot be withdrawn (MBE_ERR_INVALID). */
+int mbe_server_cancel(mbe_server* s, uint64_t request_id);
+
+int mbe_server_get_stats(mbe_server* s, mbe_server_stats* out);
+
+/* Stops the launch (graphs still on the GPU are abandoned) and frees all. */
+int mbe_server_destroy(mbe_server* s);
+
 /* ---- synthetic inputs ------------------------------------------------------
  * Seeded Chung-Lu bipartite generator (splitmix64 stream, Vose alias
  * sampling): expected degree of vertex i proportional to (i+1)^(-1/(gamma-1)),

@@ -224,7 +224,8 @@ def test_ctypes_mirrors_match_the_c_header(gm, tmp_path):
     # gcc compiles a probe against include/mbe.h that prints each struct's
     # size and every field's offset.
     mirrors = {"mbe_opts": gm.Opts, "mbe_graph_info": gm.GraphInfo, "mbe_params": gm.Params,
-               "mbe_result": gm.Result, "mbe_gen_spec": gm.GenSpec}
+               "mbe_result": gm.Result, "mbe_gen_spec": gm.GenSpec,
+               "mbe_server_config": gm.ServerConfig, "mbe_server_stats": gm.ServerStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mbe.h"', 'int main(void) {']
     for cname, py in mirrors.items():
         lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
@@ -242,3 +243,13 @@ def test_ctypes_mirrors_match_the_c_header(gm, tmp_path):
         assert int(got[cname]) == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"
+
+
+def test_server_needs_a_device(gm):
+    # Without a usable GPU the server reports a CUDA error instead of crashing.
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(gm.MBEError) as ei:
+        gm.Server()
+    assert ei.value.name == "MBE_ERR_CUDA"

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle
-from util import planted, random_bipartite
+from util import hub_graph, planted, random_bipartite
 
 pytestmark = pytest.mark.gpu
 
@@ -60,24 +60,6 @@ def test_small_config(gm):
     for uvtrans in (0, 1):
         r = run(gm, g.row_off, g.col, g.nU, opts=dict(uvtrans=uvtrans))
         assert (r.count, r.set_hash) == (want.count, want.set_hash)
-
-
-def hub_graph(seed, nV=600, nU=1200, hubs=10, hub_deg=300, p_bg=0.004):
-    """Sparse background plus a few V rows of degree ~hub_deg (|L| > 128)."""
-    rng = np.random.default_rng(seed)
-    A = rng.random((nV, nU)) < p_bg
-    for h in rng.choice(nV, size=hubs, replace=False):
-        A[h, rng.choice(nU, size=hub_deg, replace=False)] = True
-    for v in range(nV):
-        if not A[v].any():
-            A[v, rng.integers(nU)] = True
-    for u in range(nU):
-        if not A[:, u].any():
-            A[rng.integers(nV), u] = True
-    rows = [np.nonzero(A[v])[0].astype(np.int32) for v in range(nV)]
-    ro = np.zeros(nV + 1, np.int32)
-    ro[1:] = np.cumsum([len(r) for r in rows])
-    return ro, np.concatenate(rows).astype(np.int32), nU
 
 
 @pytest.mark.parametrize("seed", range(3))

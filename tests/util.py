@@ -37,3 +37,24 @@ def planted(nV, nU, blocks, seed, p_bg=0.02, p_blk=0.8, bsize=12):
     ro = np.zeros(nV + 1, np.int32)
     ro[1:] = np.cumsum([len(r) for r in rows])
     return ro, np.concatenate(rows).astype(np.int32), nU
+
+
+
+
+
+def hub_graph(seed, nV=600, nU=1200, hubs=10, hub_deg=300, p_bg=0.004):
+    """Sparse background plus a few V rows of degree ~hub_deg (|L| > 128)."""
+    rng = np.random.default_rng(seed)
+    A = rng.random((nV, nU)) < p_bg
+    for h in rng.choice(nV, size=hubs, replace=False):
+        A[h, rng.choice(nU, size=hub_deg, replace=False)] = True
+    for v in range(nV):
+        if not A[v].any():
+            A[v, rng.integers(nU)] = True
+    for u in range(nU):
+        if not A[:, u].any():
+            A[rng.integers(nV), u] = True
+    rows = [np.nonzero(A[v])[0].astype(np.int32) for v in range(nV)]
+    ro = np.zeros(nV + 1, np.int32)
+    ro[1:] = np.cumsum([len(r) for r in rows])
+    return ro, np.concatenate(rows).astype(np.int32), nU
