@@ -183,6 +183,102 @@ def run_profile_case():
                       "set_hash": f"{b.set_hash:#x}", "kernel_ms": b.kernel_ms}), flush=True)
 
 
+def batched_leg(n=4096, replays=3, plain_stride=4):
+    """Batched workload: n graphs of the batched distribution (seeds 1000..)
+    in one persistent launch replayed from a CUDA graph, against one plain
+    launch per graph on every plain_stride-th graph (graphs resident on the
+    device in both arms); per-graph results must be equal."""
+    import gmbe_b200 as gm
+    gs = [gm.batch_graph(1000 + i) for i in range(n)]
+    B = gm.Batch(gs)
+    per, tot = B.run()  # capture + warm-up
+    walls = []
+    for _ in range(replays):
+        t = time.perf_counter()
+        per, tot = B.run()
+        walls.append(time.perf_counter() - t)
+    wall = statistics.median(walls)
+    sample = list(range(0, n, plain_stride))
+    Gs = [gm.Graph.from_csr(gs[i].row_off, gs[i].col, gs[i].nU, **FLAGS) for i in sample]
+    Gs[0].enumerate()
+    t = time.perf_counter()
+    plain = [G.enumerate() for G in Gs]
+    plain_wall = time.perf_counter() - t
+    equal = all((plain[k].count, plain[k].set_hash) == (per[i].count, per[i].set_hash)
+                for k, i in enumerate(sample))
+    for G in Gs:
+        G.free()
+    B.free()
+    return {"graphs": n, "graphs_per_s": n / wall, "replay_ms": wall * 1e3,
+            "kernel_ms": tot.kernel_ms, "bicliques": tot.count,
+            "plain_graphs_per_s": len(sample) / plain_wall,
+            "plain_sample": f"every {plain_stride}th graph, one mbe_enumerate each",
+            "speedup_vs_plain": (n / wall) / (len(sample) / plain_wall),
+            "results_equal_plain": equal}
+
+
+def serving_leg(n=1000, rates=(1000, 5000, 20000)):
+    """Serving: n requests (95 % batched-distribution graphs, 5 % medium
+    serving graphs; stream seed 7) submitted at Poisson arrival times for each
+    offered load, through mbe_server_*; latency from arrival to result.  The
+    plain arm runs each request through mbe_graph_from_csr + mbe_enumerate
+    (measured service times) and its latencies are those of a FIFO server at
+    the same arrival process."""
+    import numpy as np
+    import gmbe_b200 as gm
+    from gmbe_b200.configs import serve_mix
+    reqs, is_med = serve_mix(n)
+    rng = np.random.default_rng(7)
+    pct = lambda x, q: float(np.percentile(x, q)) * 1e3
+    srv = gm.Server(max_v=32768, max_degree=4096, max_two_hop=1 << 17, arena_bytes=8 << 30,
+                    max_graphs=4096)
+    for g in reqs[:20]:
+        srv.wait(srv.submit(g.row_off, g.col, g.nU), timeout=300)
+    loads, outs = {}, []
+    arrivals = {}
+    for rate in rates:
+        arr = np.cumsum(rng.exponential(1.0 / rate, n))
+        arrivals[rate] = arr
+        t0 = time.perf_counter()
+        sub = []
+        for i, g in enumerate(reqs):
+            while time.perf_counter() - t0 < arr[i]:
+                pass
+            sub.append((srv.submit(g.row_off, g.col, g.nU), time.perf_counter() - t0))
+        lat, fin, out = [], [], []
+        for (rid, ts), a in zip(sub, arr):
+            r = srv.wait(rid, timeout=600)
+            out.append((r.count, r.set_hash))
+            lat.append(ts + r.enum_seconds - a)
+            fin.append(ts + r.enum_seconds)
+        outs.append(out)
+        loads[str(rate)] = {"graphs_per_s": n / max(fin), "p50_ms": pct(lat, 50),
+                            "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
+    st = srv.stats()
+    srv.close()
+    svc, plain = [], []
+    for g in reqs:
+        t = time.perf_counter()
+        with gm.Graph.from_csr(g.row_off, g.col, g.nU, **FLAGS) as G:
+            r = G.enumerate()
+        svc.append(time.perf_counter() - t)
+        plain.append((r.count, r.set_hash))
+    for rate in rates:
+        fin, lat = 0.0, []
+        for a, s in zip(arrivals[rate], svc):
+            fin = max(fin, a) + s
+            lat.append(fin - a)
+        loads[str(rate)]["plain_fifo"] = {"graphs_per_s": n / fin, "p50_ms": pct(lat, 50),
+                                          "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
+    plain_gps = n / sum(svc)
+    best = max(v["graphs_per_s"] for v in loads.values())
+    return {"requests": n, "medium_requests": int(is_med.sum()),
+            "mix": "95% batched-distribution graphs, 5% 20k x 80k ~300k-edge graphs; Poisson arrivals, seed 7",
+            "loads_per_s": loads, "plain_graphs_per_s": plain_gps,
+            "speedup_vs_plain": best / plain_gps, "launches": st["launches"],
+            "results_equal_plain": all(o == plain for o in outs)}
+
+
 def WORKLOAD_DESC():
     import gmbe_b200 as gm
     return gm.DESCRIPTIONS[WORKLOAD]
@@ -195,6 +291,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and serving legs (they run at N=1 only)")
     ap.add_argument("--profile", action="store_true",
                     help="one reduced launch for ncu: 16 blocks, every 64th root (~1.6 GB scratch)")
     args = ap.parse_args()
@@ -318,6 +416,9 @@ def main():
                          "algorithmic_bytes_per_launch": alg,
                          "kernel": "mbe_enum_kernel"},
         }
+        if world == 1 and not args.no_extras:
+            line["batched"] = batched_leg()
+            line["serving"] = serving_leg()
         if world == 1 and not args.no_cpu_baseline:
             v, sample, cores = cpu_sample(g)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",

@@ -58,7 +58,8 @@ class Params(C.Structure):
                 ("sm_timing", C.c_int32), ("root_begin", C.c_int32), ("root_end", C.c_int32),
                 ("shard_count", C.c_int32), ("shard_index", C.c_int32),
                 ("split_mode", C.c_int32), ("direct_max_c", C.c_int32),
-                ("root_split_size", C.c_int32), ("share_min_work", C.c_int32)]
+                ("root_split_size", C.c_int32), ("share_min_work", C.c_int32),
+                ("range_split_work", C.c_int32), ("range_chunk", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -72,7 +73,10 @@ class Result(C.Structure):
                 ("max_task_degree", C.c_int32), ("n_tasks", C.c_uint64),
                 ("n_subproblems", C.c_uint64), ("max_task_tier1_ms", C.c_double),
                 ("max_task_tier2_ms", C.c_double), ("max_task_graph", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("reserved", C.c_int32), ("max_task_pushes1", C.c_uint64),
+                ("max_task_pushes2", C.c_uint64), ("max_task_cands", C.c_int32),
+                ("max_task_part", C.c_int32), ("max_task_parts", C.c_int32),
+                ("reserved2", C.c_int32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -54,3 +54,19 @@ def config_graph(name: str):
 def batch_graph(seed: int):
     """One graph of the batched workload (seeds 1000..5095)."""
     return generate(batch_spec(seed))
+
+
+def serve_mix(n: int, seed: int = 7, medium_share: float = 0.05, medium_pool: int = 4):
+    """The serving request stream: n graphs, each a medium serving graph
+    (20,000 x 80,000, ~300,000 edges, exponent 2.1) with probability
+    medium_share, else a graph of the batched distribution (seed 1000 + i).
+    The medium requests cycle through medium_pool seeded graphs.  Returns
+    (graphs, is_medium)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    med = [generate(_spec(20000, 80000, 300000, 2.1, 2.1, 2000, 2000, seed * 1000 + k))
+           for k in range(medium_pool)]
+    is_med = rng.random(n) < medium_share
+    graphs = [med[i % medium_pool] if is_med[i] else batch_graph(1000 + i) for i in range(n)]
+    return graphs, is_med
+

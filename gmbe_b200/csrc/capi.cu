@@ -183,6 +183,8 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   s.act_cap = (int32_t)std::min<int64_t>(INT32_MAX / 2, 6 * C + 8192);
   s.act = take(s.act_cap);
   s.words_per_warp = off;
+  const int64_t seen = ((int64_t)nV + 31) / 32;
+  s.seen_words = seen <= kSeenMaxWords ? (int32_t)seen : 0;
   return s;
 }
 
@@ -194,7 +196,7 @@ int apply_tuning(const mbe_params& prm, DevGraph* dg) {
   dg->bound_height = prm.bound_height;
   dg->bound_size = prm.bound_size;
   dg->tier2_max_l = t2;
-  dg->direct_max_c = prm.direct_max_c > 0 ? prm.direct_max_c : 4096;
+  dg->direct_max_c = prm.direct_max_c > 0 ? prm.direct_max_c : 16384;
   return MBE_OK;
 }
 
@@ -213,6 +215,8 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   if (spec.capC >= (1 << 24))
     return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
   plan->sl = make_layout(spec.map_words, spec.capC, spec.capL, spec.capS);
+  CK(cudaFuncSetAttribute(mbe_enum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)enum_smem_bytes(plan->sl)));
   plan->map_words = spec.map_words;
   size_t need = (size_t)plan->sl.words_per_warp * (size_t)plan->warps * sizeof(int32_t);
   if (need > ws.scratch_bytes) {
@@ -280,6 +284,7 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   // Heavy roots split into vertex tuples (sub-problem sharing mode only).
   ep.root_split = prm.split_mode == 1 ? 0 : std::max(prm.root_split_size, 0);
   ep.share_min_work = prm.share_min_work > 0 ? prm.share_min_work : kShareMinWorkDefault;
+  apply_range_split(prm, &ep.range_work, &ep.range_chunk);
   ep.n_graphs = spec.n_graphs;
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;
@@ -309,7 +314,7 @@ int engine_enqueue(Workspace& ws, LaunchPlan* plan, const DevGraph* d_graphs,
   CK(cudaMemsetAsync(ws.slot_bits, 0, sizeof(uint32_t) * (size_t)(ws.nslot / 32), st));
   CK(cudaMemsetAsync(d_gres, 0, 3 * sizeof(unsigned long long) * (size_t)n_graphs, st));
   if (ev0) CK(cudaEventRecord(ev0, st));
-  mbe_enum_kernel<<<plan->blocks, kEnumThreads, 0, st>>>(d_graphs, d_prefix, d_gres, plan->ep,
+  mbe_enum_kernel<<<plan->blocks, kEnumThreads, enum_smem_bytes(plan->sl), st>>>(d_graphs, d_prefix, d_gres, plan->ep,
                                                           plan->sl, ws.ctl, ws.q_tasks, ws.q_seq,
                                                           plan->pool, ws.scratch, ws.exit_ns);
   CK(cudaGetLastError());
@@ -345,6 +350,11 @@ void fill_profile(const EnumCtl& ctl, mbe_result* out) {
   out->max_task_degree = (int32_t)(ctl.max_task_info & 0xffffffffu);
   out->max_task_tier1_ms = (double)(ctl.max_task_split & 0xffffffffu) / 1e3;
   out->max_task_tier2_ms = (double)(ctl.max_task_split >> 32) / 1e3;
+  out->max_task_pushes1 = ctl.max_task_pushes & 0xffffffffu;
+  out->max_task_pushes2 = ctl.max_task_pushes >> 32;
+  out->max_task_cands = (int32_t)(ctl.max_task_shape & 0xffffffffu);
+  out->max_task_part = (int32_t)((ctl.max_task_shape >> 32) & 0xffff);
+  out->max_task_parts = (int32_t)(ctl.max_task_shape >> 48);
   out->max_task_graph = (int32_t)ctl.max_task_graph;
   out->n_tasks = ctl.n_tasks;
   out->n_subproblems = ctl.n_tier2;

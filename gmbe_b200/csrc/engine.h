@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "enum_launch.h"
@@ -79,6 +80,12 @@ int engine_status(Workspace& ws, const EnumCtl& ctl);
 
 // Copies the profile counters of the control block into a result.
 void fill_profile(const EnumCtl& ctl, mbe_result* out);
+
+// Root splitting settings of a launch from the parameters.
+inline void apply_range_split(const mbe_params& prm, int32_t* work, int32_t* chunk) {
+  *work = prm.split_mode == 1 ? 0 : std::max(prm.range_split_work, 0);
+  *chunk = prm.range_chunk > 0 ? prm.range_chunk : kRangeChunkDefault;
+}
 
 // Per-graph tuning fields of a descriptor from parameters.
 int apply_tuning(const mbe_params& prm, DevGraph* dg);

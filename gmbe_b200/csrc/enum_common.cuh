@@ -37,7 +37,10 @@ struct DevGraph {
 struct alignas(16) Task {
   int32_t v[4];
   int32_t graph;  // index into the launch's graph array
-  int32_t pad[3];
+  // A root split into `parts` parts (0 = whole): part j pushes, at its first
+  // level, only the candidates whose vertex hashes to bucket j.
+  int32_t part, parts;
+  int32_t pad;
 };
 
 // Global control block (one per launch).
@@ -64,6 +67,8 @@ struct EnumCtl {
   unsigned long long max_task_info; // (root << 32) | |L| of that task
   unsigned long long max_task_split; // its counts-tier us | bitmap-tier us << 32
   unsigned long long max_task_graph; // its graph
+  unsigned long long max_task_pushes; // its pushes: counts tier | bitmap tier << 32
+  unsigned long long max_task_shape;  // its |C| | part << 32 | parts << 48 (root tasks)
   unsigned long long n_tasks, n_tier2;
 };
 
@@ -80,7 +85,10 @@ struct ScratchLayout {
   int64_t lkey, lmask;  // lkey is uint64 (8-byte aligned offset)
   int64_t t2_rec, t2_n, t2_cur, t2_top, r_sum, r_cnt;  // bitmap-tier stack; t2_rec, r_sum uint64
   int64_t act, tlist;
-  int32_t act_cap, pad;
+  int32_t act_cap;
+  // Words per warp of the first-touch bitmap in shared memory (one bit per
+  // V vertex / candidate position); 0 = first touches found by global atomics.
+  int32_t seen_words;
 };
 
 // Slots for bitmap sub-problems handed to idle warps.
@@ -139,6 +147,8 @@ struct EnumParams {
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)
   int32_t root_split;         // > 0: a root task with |P|*|L| above this splits into vertex tuples
   int32_t share_min_work;     // |P|*|L| of a child shared out while many warps wait
+  int32_t range_work;         // > 0: a root with |P|*|L| above this is split into parts
+  int32_t range_chunk;        // P candidates per part
   int32_t server;             // 1: graphs arrive while the launch runs (ServeLink)
   ServeLink serve;
 };

@@ -90,11 +90,39 @@ struct Warp {
   // accumulators (uniform over lanes)
   unsigned long long cnt, hash, nonmax, splits;
   unsigned long long ns_t2, n_t2;  // time inside the bitmap tier, sub-problems run
+  unsigned long long pushes;       // pushes so far: counts tier | bitmap tier << 32
+  unsigned long long shape;        // last task set up: |C| | (part << 32) | (parts << 48)
   unsigned long long ns_t1;        // time inside the counts tier (bitmap tier excluded)
+  uint32_t* seen;                  // this warp's first-touch bitmap in shared memory, or null
 
   __device__ int32_t* A(int64_t off) const { return base + off; }
   __device__ uint64_t* A64(int64_t off) const { return reinterpret_cast<uint64_t*>(base + off); }
 };
+
+// Adds 1 to counts[i] and tells whether this was i's first touch since the
+// counts were last cleared.  With a shared-memory bitmap the first touch is a
+// shared atomic and the count a fire-and-forget global one, so the warp does
+// not wait for an L2 round trip per entry; without it, the returned old count
+// tells.
+__device__ __forceinline__ bool count_first(const Warp& W, int32_t* counts, int i) {
+  if (W.seen) {
+    const uint32_t bit = 1u << (i & 31);
+    atomicAdd(&counts[i], 1);
+    return (atomicOr(&W.seen[i >> 5], bit) & bit) == 0u;
+  }
+  return atomicAdd(&counts[i], 1) == 0;
+}
+
+// After a counting pass: makes every lane's count increments visible to the
+// warp, and clears the bitmap bits of the `n` indices touched (listed in idx).
+__device__ __forceinline__ void counts_done(const Warp& W, const int32_t* idx, int n) {
+  __threadfence_block();
+  __syncwarp();
+  if (W.seen) {
+    for (int i = (int)lane_id(); i < n; i += 32) W.seen[idx[i] >> 5] = 0u;
+    __syncwarp();
+  }
+}
 
 // Serving block of graph `gid` (a block index into the arena, which the
 // launch receives in place of the descriptor array).
@@ -106,6 +134,15 @@ __device__ __forceinline__ ServeGraph* serve_graph(const Warp& W, int32_t gid) {
 // Descriptor of graph `gid` of this launch.
 __device__ __forceinline__ const DevGraph* graph_at(const Warp& W, int32_t gid) {
   return W.p.server ? &serve_graph(W, gid)->g : W.graphs + gid;
+}
+
+// Most parts a root is split into.
+constexpr int kMaxParts = 1024;
+
+// Bucket of candidate w among `parts` (Knuth's multiplicative hash, scaled):
+// spreads consecutive ids, hence the work, evenly over the parts.
+__device__ __forceinline__ int part_of(int w, int parts) {
+  return (int)(((unsigned long long)((uint32_t)w * 2654435761u) * (unsigned)parts) >> 32);
 }
 
 // Children of the current graph about to be queued (serving: a graph
@@ -132,6 +169,7 @@ struct T2Src {
   const uint64_t* lkey;
   uint32_t L0[4];          // the sub-problem's L
   int nsub, nq;            // records [0, nq) are Q, [nq, nsub) P
+  int nend;                // the first level pushes records [nq, nend) only
   uint64_t sR0;            // R of the sub-problem's root biclique
   uint32_t nR0;
 };
@@ -214,6 +252,7 @@ __device__ bool slot_publish(Warp& W, int slot) {
   Task t;
   t.v[0] = -2 - slot;
   t.v[1] = t.v[2] = t.v[3] = -1;
+  t.graph = t.part = t.parts = t.pad = 0;
   return queue_push_one(W, t);
 }
 
@@ -316,10 +355,11 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
 #pragma unroll
     for (int w = 0; w < K; ++w) Lm[w] = lmask[(level - 1) * K + w];
     int cp = -1;
-    for (int b0 = lcur[level - 1]; b0 < n; b0 += 32) {
+    const int e = level == 1 ? src.nend : n;  // the first level may push a part only
+    for (int b0 = lcur[level - 1]; b0 < e; b0 += 32) {
       int q = b0 + lane;
       bool ok = false;
-      if (q < n) {
+      if (q < e) {
         const uint32_t* r = R + (size_t)q * RS;
         if ((int)(r[0] & 0xffu) > level - 1) {
           uint32_t any = 0;
@@ -336,6 +376,7 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
     }
     if (cp >= 0) {
       // ---- push (finder_push) ----
+      W.pushes += 1ULL << 32;
       uint32_t Ln[K];
       int kn = 0;
 #pragma unroll
@@ -350,40 +391,57 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
       uint64_t sR = 0;
       unsigned long long nR = 0;
       int nchild = 0, nbefore = 0;
-      for (int b0 = 0; b0 < n; b0 += 32) {
-        int q = b0 + lane;
-        bool keep = false;
-        uint32_t h = 0, m[K];
-        if (q < n) {
-          uint32_t* r = R + (size_t)q * RS;
-          h = r[0];
-          bool cover = true, meet = false;
+      // The pass is bound by load latency: each lane loads U records before
+      // any of them is used, so U loads per lane are in flight at once.
+      constexpr int U = K <= 2 ? 4 : 2;
+      for (int b0 = 0; b0 < n; b0 += 32 * U) {
+        uint32_t hu[U], mu[U][K];
 #pragma unroll
-          for (int w = 0; w < K; ++w) {
-            m[w] = r[1 + w];
-            uint32_t x = m[w] & Ln[w];
-            cover &= x == Ln[w];
-            meet |= x != 0;
-          }
-          int b = (int)(h & 0xffu);
-          if (cover) {
-            sR += subkey[h >> 8];
-            ++nR;
-            if (q < cp && b >= level) ism = false;
-            else if (b > level) r[0] = (h & ~0xffu) | (uint32_t)level;
-          } else {
-            keep = meet && b > level;
+        for (int u = 0; u < U; ++u) {
+          const int q = b0 + u * 32 + lane;
+          hu[u] = 0u;
+#pragma unroll
+          for (int w = 0; w < K; ++w) mu[u][w] = 0u;
+          if (q < n) {
+            const uint32_t* r = R + (size_t)q * RS;
+            hu[u] = r[0];
+#pragma unroll
+            for (int w = 0; w < K; ++w) mu[u][w] = r[1 + w];
           }
         }
-        unsigned bal = __ballot_sync(kFull, keep);
-        if (fits && keep) {
-          uint32_t* c = child + (size_t)(nchild + __popc(bal & lanemask_lt())) * RS;
-          c[0] = (h & ~0xffu) | kB8Free;
 #pragma unroll
-          for (int w = 0; w < K; ++w) c[1 + w] = m[w];
+        for (int u = 0; u < U; ++u) {
+          const int q = b0 + u * 32 + lane;
+          const uint32_t h = hu[u];
+          bool keep = false;
+          if (q < n) {
+            bool cover = true, meet = false;
+#pragma unroll
+            for (int w = 0; w < K; ++w) {
+              uint32_t x = mu[u][w] & Ln[w];
+              cover &= x == Ln[w];
+              meet |= x != 0;
+            }
+            int b = (int)(h & 0xffu);
+            if (cover) {
+              sR += subkey[h >> 8];
+              ++nR;
+              if (q < cp && b >= level) ism = false;
+              else if (b > level) R[(size_t)q * RS] = (h & ~0xffu) | (uint32_t)level;
+            } else {
+              keep = meet && b > level;
+            }
+          }
+          unsigned bal = __ballot_sync(kFull, keep);
+          if (fits && keep) {
+            uint32_t* c = child + (size_t)(nchild + __popc(bal & lanemask_lt())) * RS;
+            c[0] = (h & ~0xffu) | kB8Free;
+#pragma unroll
+            for (int w = 0; w < K; ++w) c[1 + w] = mu[u][w];
+          }
+          nchild += __popc(bal);
+          nbefore += __popc(__ballot_sync(kFull, keep && q < cp));
         }
-        nchild += __popc(bal);
-        nbefore += __popc(__ballot_sync(kFull, keep && q < cp));
       }
       ism = __all_sync(kFull, ism);
       sR = warp_sum(sR) + rsum[level - 1];
@@ -450,19 +508,30 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
 #pragma unroll
       for (int w = 0; w < K; ++w)
         rem[w] = lmask[(level - 1) * K + w] & ~R2[(size_t)cp * RS + 1 + w];
-      for (int q = lane; q < n2; q += 32) {
-        uint32_t* r = R2 + (size_t)q * RS;
-        uint32_t h = r[0];
-        int b = (int)(h & 0xffu);
-        if (b >= level) {
-          uint32_t nb = kB8Free;
-          if (prune) {
-            uint32_t t = 0;
+      constexpr int UP = K <= 2 ? 4 : 2;  // records per lane in flight, as in the push
+      for (int q0 = lane; q0 < n2; q0 += 32 * UP) {
+        uint32_t hu[UP], tu[UP];
 #pragma unroll
-            for (int w = 0; w < K; ++w) t |= r[1 + w] & rem[w];
-            nb = (t != 0 || q == cp) ? kB8Free : (uint32_t)(level - 1);
+        for (int u = 0; u < UP; ++u) {
+          const int q = q0 + u * 32;
+          hu[u] = 0u;
+          tu[u] = 0u;
+          if (q < n2) {
+            const uint32_t* r = R2 + (size_t)q * RS;
+            hu[u] = r[0];
+#pragma unroll
+            for (int w = 0; w < K; ++w) tu[u] |= r[1 + w] & rem[w];
           }
-          r[0] = (h & ~0xffu) | nb;
+        }
+#pragma unroll
+        for (int u = 0; u < UP; ++u) {
+          const int q = q0 + u * 32;
+          const uint32_t h = hu[u];
+          if (q < n2 && (int)(h & 0xffu) >= level) {
+            uint32_t nb = kB8Free;
+            if (prune) nb = (tu[u] != 0 || q == cp) ? kB8Free : (uint32_t)(level - 1);
+            R2[(size_t)q * RS] = (h & ~0xffu) | nb;
+          }
         }
       }
     }
@@ -493,7 +562,7 @@ __device__ __forceinline__ void full_mask(uint32_t* L0, int n) {
 }
 
 // Sub-problem built in the warp's own scratch over n L vertices (all bits).
-__device__ void tier2(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t nR0) {
+__device__ void tier2(Warp& W, int n, int nsub, int nq, int nend, uint64_t sR0, uint64_t nR0) {
   T2Src src;
   src.rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
   src.subkey = W.A64(W.sl.sub_v);
@@ -501,6 +570,7 @@ __device__ void tier2(Warp& W, int n, int nsub, int nq, uint64_t sR0, uint64_t n
   full_mask(src.L0, n);
   src.nsub = nsub;
   src.nq = nq;
+  src.nend = nend;
   src.sR0 = sR0;
   src.nR0 = (uint32_t)nR0;
   tier2_dispatch(W, src, words_k(n));
@@ -519,6 +589,7 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   const int K = sp[0];
   src.nsub = sp[1];
   src.nq = sp[2];
+  src.nend = src.nsub;
   W.gid = sp[3];
   W.gp = graph_at(W, W.gid);
   for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)sp[4 + w];
@@ -550,6 +621,7 @@ __device__ void init_records(uint32_t* rec, int K, int nsub) {
 struct T1 {
   const int32_t* L;   // L vertices (internal U ids)
   int nL, nC, nq;
+  int nend;  // the first level pushes positions [nq, nend) only
   uint64_t sRtask, nRtask;
 };
 
@@ -683,7 +755,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
           if (s >= 0) atomicOr(&rec[(size_t)s * RS + 1 + (r >> 5)], 1u << (r & 31));
         });
     __syncwarp();
-    tier2(W, n, nsub, nq, sR, nR);
+    tier2(W, n, nsub, nq, nsub, sR, nR);
   }
   __syncwarp();
 }
@@ -745,12 +817,12 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       [&](bool valid, int, int pos) {
         int p = valid ? aadj[pos] : -1;
         bool first = false;
-        if (p >= 0) first = atomicAdd(&cc[p], 1) == 0;
+        if (p >= 0) first = count_first(W, cc, p);
         unsigned bal = __ballot_sync(kFull, first);
         if (first) tl[nt + __popc(bal & lanemask_lt())] = p;
         nt += __popc(bal);
       });
-  __syncwarp();
+  counts_done(W, tl, nt);
   // R of the child, maximality, and the child's candidates (Q part first)
   bool ism = true;
   uint64_t sR = 0;
@@ -844,7 +916,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       }
       if (!slot_publish(W, slot)) tier2_from_slot(W, slot);  // ring full: run it here
     } else {
-      tier2(W, n, ncand, nq, sR, nR);
+      tier2(W, n, ncand, nq, ncand, sR, nR);
     }
   }
   __syncwarp();
@@ -882,9 +954,10 @@ __device__ void tier1_run(Warp& W, const T1& t) {
     int ab = lane == 0 ? *(volatile int32_t*)&W.ctl->abort : 0;
     if (__shfl_sync(kFull, ab, 0)) return;
     int cur = -1;
-    for (int b0 = stack[level - 1]; b0 < t.nC; b0 += 32) {
+    const int end = level == 1 ? t.nend : t.nC;  // the first level may push a part only
+    for (int b0 = stack[level - 1]; b0 < end; b0 += 32) {
       int i = b0 + lane;
-      bool ok = i < t.nC && bound[i] > level - 1 && ncnt[i] != 0;
+      bool ok = i < end && bound[i] > level - 1 && ncnt[i] != 0;
       unsigned bal = __ballot_sync(kFull, ok);
       if (bal) {
         cur = b0 + __ffs(bal) - 1;
@@ -893,6 +966,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
     }
     if (cur >= 0) {
       // ---- finder_push (src/IterFinderGpu.h:206-264) ----
+      W.pushes += 1;
       int kept = 0;
       uint64_t sL = 0;
       int rb = coff[cur], re = coff[cur + 1];
@@ -1023,18 +1097,21 @@ __device__ bool queue_pop(Warp& W, Task* out) {
   out->v[2] = src[2];
   out->v[3] = src[3];
   out->graph = src[4];
+  out->part = src[5];
+  out->parts = src[6];
   __threadfence();
   atomicExch(W.q_seq + slot, full + 1);  // free for round h/cap + 1
   atomicAdd(&ctl->q_used, (unsigned long long)-1LL);
   return true;
 }
 
-// Pushes children task + {cv[i]} for i in [nq, nC); false if the ring is full.
-__device__ bool queue_push_children(Warp& W, const Task& t, int k, int nq, int nC) {
+// Queues n tasks, task i (0 <= i < n) made by make(i); false if the ring is
+// full (then nothing is queued).
+template <typename Make>
+__device__ bool queue_push_n(Warp& W, unsigned long long n, Make make) {
   const int lane = (int)lane_id();
   EnumCtl* ctl = W.ctl;
   const int cap = W.p.queue_cap;
-  unsigned long long n = (unsigned long long)(nC - nq);
   unsigned long long pos = 0;
   int ok = 0;
   if (lane == 0) {
@@ -1051,9 +1128,8 @@ __device__ bool queue_push_children(Warp& W, const Task& t, int k, int nq, int n
   ok = __shfl_sync(kFull, ok, 0);
   if (!ok) return false;
   pos = __shfl_sync(kFull, pos, 0);
-  const int32_t* cv = W.A(W.sl.cv);
-  for (int i = nq + lane; i < nC; i += 32) {
-    unsigned long long gp = pos + (unsigned long long)(i - nq);
+  for (unsigned long long i = lane; i < n; i += 32) {
+    unsigned long long gp = pos + i;
     unsigned long long slot = gp % (unsigned long long)cap;
     volatile unsigned long long* st = W.q_seq + slot;
     const unsigned long long free_tag = slot_free_tag(gp, cap);
@@ -1068,14 +1144,33 @@ __device__ bool queue_push_children(Warp& W, const Task& t, int k, int nq, int n
       __nanosleep(64);
     }
     if (!ready) continue;  // the run is aborting; the slot stays unwritten
-    Task c = t;
-    c.v[k] = cv[i];
-    W.q_tasks[slot] = c;
+    W.q_tasks[slot] = make((int)i);
     __threadfence();
     atomicExch(W.q_seq + slot, free_tag + 1);
   }
   __syncwarp();
   return true;
+}
+
+// Pushes children task + {cv[i]} for i in [nq, nC); false if the ring is full.
+__device__ bool queue_push_children(Warp& W, const Task& t, int k, int nq, int nC) {
+  const int32_t* cv = W.A(W.sl.cv);
+  return queue_push_n(W, (unsigned long long)(nC - nq), [&](int i) {
+    Task c = t;
+    c.v[k] = cv[nq + i];
+    c.part = c.parts = 0;
+    return c;
+  });
+}
+
+// Pushes parts 1 .. m-1 of root task t; false if the ring is full.
+__device__ bool queue_push_parts(Warp& W, const Task& t, int m) {
+  return queue_push_n(W, (unsigned long long)(m - 1), [&](int i) {
+    Task c = t;
+    c.part = i + 1;
+    c.parts = m;
+    return c;
+  });
 }
 
 // Pushes one task (lane-uniform); false if the ring is full.
@@ -1202,13 +1297,12 @@ __device__ void run_task(Warp& W, const Task& t) {
       },
       [&](bool valid, int, int pos) {
         int w = valid ? __ldg(g.rev_col + pos) : 0;
-        int old = valid ? atomicAdd(&map[w], 1) : 1;
-        bool isnew = valid && old == 0;
+        bool isnew = valid && count_first(W, map, w);
         unsigned bal = __ballot_sync(kFull, isnew);
         if (isnew) touched[nt + __popc(bal & lanemask_lt())] = w;
         nt += __popc(bal);
       });
-  __syncwarp();
+  counts_done(W, touched, min(nt, W.sl.capC));
   if (nt > W.sl.capC) {
     set_status(W.ctl, kStCapacity, ((unsigned long long)3 << 32) | (unsigned)nt);
     for (int i = lane; i < nt && i < W.sl.capC; i += 32) map[touched[i]] = 0;
@@ -1221,47 +1315,101 @@ __device__ void run_task(Warp& W, const Task& t) {
   int32_t* bound = W.A(W.sl.bound);
   uint64_t sR = 0;
   unsigned long long nR = 0;
-  int nq = 0, np = 0;
+  int nq = 0, np = 0, nend = 0;
   int viol_first = 0x7fffffff;  // smallest R vertex below `last` (maximality witnesses)
   int nC = 0;
+  // C is laid out [Q | P before this part | P of this part | P after it]; a
+  // task that is not a part has only the middle P group.  The first level
+  // pushes the candidates of this part; those before it act as Q, those after
+  // it stay candidates of the children.
+  int part = t.part, parts = t.parts;
+  int cntQ = 0, cntPre = 0, cntIn = 0;
   {
-    // count C size first so P can fill from the back
     int cntC = 0;
+    bool r_below = false;
     for (int b0 = 0; b0 < nt; b0 += 32) {
       int i = b0 + lane;
-      bool isC = i < nt && map[touched[i]] != nL;
+      bool valid = i < nt;
+      int w = valid ? touched[i] : 0;
+      int c = valid ? map[w] : 0;
+      bool isC = valid && c != nL;
       cntC += __popc(__ballot_sync(kFull, isC));
+      cntQ += __popc(__ballot_sync(kFull, isC && w < last));
+      r_below |= __ballot_sync(kFull, valid && c == nL && w < last) != 0u;
     }
     nC = cntC;
+    const int np_all = cntC - cntQ;
+    // A heavy maximal root is split into parts before its C is laid out.
+    // Its first level costs about |P| pushes, each a pass over all of C.
+    if (k == 1 && parts == 0 && !r_below && W.p.range_work > 0 &&
+        np_all >= 2 * W.p.range_chunk &&
+        (long long)np_all * cntC > (long long)W.p.range_work) {
+      const int m = min((np_all + W.p.range_chunk - 1) / W.p.range_chunk, kMaxParts);
+      if (queue_push_parts(W, t, m)) {
+        part = 0;
+        parts = m;
+        W.splits += 1;
+      }
+    }
+    if (parts > 1) {
+      for (int b0 = 0; b0 < nt; b0 += 32) {
+        int i = b0 + lane;
+        bool valid = i < nt;
+        int w = valid ? touched[i] : 0;
+        bool isP = valid && map[w] != nL && w > last;
+        int b = isP ? part_of(w, parts) : 0;
+        cntPre += __popc(__ballot_sync(kFull, isP && b < part));
+        cntIn += __popc(__ballot_sync(kFull, isP && b == part));
+      }
+    } else {
+      cntIn = np_all;
+    }
   }
-  for (int b0 = 0; b0 < nt; b0 += 32) {
-    int i = b0 + lane;
-    bool valid = i < nt;
-    int w = valid ? touched[i] : 0;
-    int c = valid ? map[w] : 0;
-    bool isR = valid && c == nL;
-    bool isQ = valid && !isR && w < last;
-    bool isP = valid && !isR && w > last;
-    if (isR) {
-      sR += g.vkey[w];
-      ++nR;
-      if (w < last) viol_first = min(viol_first, w);
+  {
+    int oQ = 0, oPre = cntQ, oIn = cntQ + cntPre, oPost = cntQ + cntPre + cntIn;
+    for (int b0 = 0; b0 < nt; b0 += 32) {
+      int i = b0 + lane;
+      bool valid = i < nt;
+      int w = valid ? touched[i] : 0;
+      int c = valid ? map[w] : 0;
+      bool isR = valid && c == nL;
+      bool isQ = valid && !isR && w < last;
+      bool isP = valid && !isR && w > last;
+      int b = (isP && parts > 1) ? part_of(w, parts) : part;
+      bool isPre = isP && b < part, isIn = isP && b == part, isPost = isP && b > part;
+      if (isR) {
+        sR += g.vkey[w];
+        ++nR;
+        if (w < last) viol_first = min(viol_first, w);
+      }
+      unsigned bq = __ballot_sync(kFull, isQ);
+      unsigned bpre = __ballot_sync(kFull, isPre);
+      unsigned bin = __ballot_sync(kFull, isIn);
+      unsigned bpost = __ballot_sync(kFull, isPost);
+      const unsigned lt = lanemask_lt();
+      int pos = -1;
+      if (isQ) pos = oQ + __popc(bq & lt);
+      if (isPre) pos = oPre + __popc(bpre & lt);
+      if (isIn) pos = oIn + __popc(bin & lt);
+      if (isPost) pos = oPost + __popc(bpost & lt);
+      if (pos >= 0) {
+        cv[pos] = w;
+        ncnt[pos] = c;
+        bound[pos] = kFree;
+        map[w] = pos + 1;
+      } else if (valid) {
+        map[w] = 0;
+      }
+      oQ += __popc(bq);
+      oPre += __popc(bpre);
+      oIn += __popc(bin);
+      oPost += __popc(bpost);
     }
-    unsigned bq = __ballot_sync(kFull, isQ);
-    unsigned bp = __ballot_sync(kFull, isP);
-    int pos = -1;
-    if (isQ) pos = nq + __popc(bq & lanemask_lt());
-    if (isP) pos = nC - 1 - (np + __popc(bp & lanemask_lt()));
-    if (pos >= 0) {
-      cv[pos] = w;
-      ncnt[pos] = c;
-      bound[pos] = kFree;
-      map[w] = pos + 1;
-    } else if (valid) {
-      map[w] = 0;
-    }
-    nq += __popc(bq);
-    np += __popc(bp);
+    nq = cntQ + cntPre;  // first P position this task pushes
+    np = cntIn;
+    nend = nq + cntIn;
+    W.shape = (unsigned long long)(unsigned)nC | ((unsigned long long)(part & 0xffff) << 32) |
+              ((unsigned long long)(parts & 0xffff) << 48);
   }
   sR = warp_sum(sR);
   nR = warp_sum(nR);
@@ -1338,8 +1486,8 @@ __device__ void run_task(Warp& W, const Task& t) {
     __syncwarp();
     return;
   }
-  // the task's own biclique
-  {
+  // the task's own biclique (once: parts after the first skip it)
+  if (part == 0) {
     uint64_t sL = 0;
     for (int l = lane; l < nL; l += 32) sL += g.ukey[L[l]];
     sL = warp_sum(sL);
@@ -1357,7 +1505,8 @@ __device__ void run_task(Warp& W, const Task& t) {
       split = (rest > W.gp->bound_height || nL > W.gp->bound_height) &&
               rest * (long long)nL > (long long)W.gp->bound_size;
     else
-      split = k == 1 && W.p.root_split > 0 && rest * (long long)nL > (long long)W.p.root_split;
+      split = k == 1 && parts <= 1 && W.p.root_split > 0 &&
+              rest * (long long)nL > (long long)W.p.root_split;
     if (split) {
       if (queue_push_children(W, t, k, nq, nC)) {
         W.splits += 1;
@@ -1388,7 +1537,7 @@ __device__ void run_task(Warp& W, const Task& t) {
             if (p >= 0) atomicOr(&rec[(size_t)p * RS + 1 + (r >> 5)], 1u << (r & 31));
           });
       __syncwarp();
-      tier2(W, nL, nC, nq, sR, nR);
+      tier2(W, nL, nC, nq, nend, sR, nR);
     } else {
       // ---- tier 1: local adjacency ----
       int32_t* llevel = W.A(W.sl.llevel);
@@ -1453,6 +1602,7 @@ __device__ void run_task(Warp& W, const Task& t) {
       t1.nL = nL;
       t1.nC = nC;
       t1.nq = nq;
+      t1.nend = nend;
       t1.sRtask = sR;
       t1.nRtask = nR;
       uint64_t t1s = globaltimer_ns();
@@ -1506,6 +1656,7 @@ __device__ bool serve_claim_root(Warp& W, Task* t) {
       t->v[0] = g.root_end - 1 - (g.root_offset + (int)r * g.root_stride);
       t->v[1] = t->v[2] = t->v[3] = -1;
       t->graph = (int32_t)blk;
+      t->part = t->parts = t->pad = 0;
       return true;
     }
     atomicCAS((unsigned long long*)&L.sctl->arr_head, h, h + 1);
@@ -1551,12 +1702,20 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   W.slot_bits = pool.bits;
   W.nslot = pool.nslot;
   W.base = scratch + (size_t)warp_global * (size_t)sl.words_per_warp;
+  extern __shared__ uint32_t enum_smem[];
+  W.seen = sl.seen_words ? enum_smem + (size_t)(threadIdx.x >> 5) * sl.seen_words : nullptr;
+  if (W.seen) {
+    for (int i = lane; i < sl.seen_words; i += 32) W.seen[i] = 0u;
+    __syncwarp();
+  }
   W.graphs = graphs;
   W.gp = graphs;
   W.gid = 0;
   W.cnt = W.hash = W.nonmax = W.splits = 0;
   W.ns_t1 = W.ns_t2 = W.n_t2 = 0;
+  W.pushes = W.shape = 0;
   uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0, max_split = 0;
+  uint64_t max_pushes = 0, max_shape = 0;
   int32_t max_gid = 0;
   const long long nroots = p.server ? 0 : root_prefix[p.n_graphs];
   uint64_t idle_since = 0;
@@ -1584,6 +1743,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
           t.v[0] = gg.root_end - 1 - (int)(gg.root_offset + k * gg.root_stride);
           t.v[1] = t.v[2] = t.v[3] = -1;
           t.graph = gi;
+          t.part = t.parts = t.pad = 0;
           have = 1;
         } else {
           atomicAdd(&ctl->pending, (unsigned long long)-1LL);
@@ -1595,9 +1755,12 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
 #pragma unroll
       for (int i = 0; i < 4; ++i) t.v[i] = __shfl_sync(kFull, t.v[i], 0);
       t.graph = __shfl_sync(kFull, t.graph, 0);
+      t.part = __shfl_sync(kFull, t.part, 0);
+      t.parts = __shfl_sync(kFull, t.parts, 0);
       if (idle_since != 0 && lane == 0) atomicSub(&ctl->idle_warps, 1);
       uint64_t tb = globaltimer_ns();
       const unsigned long long t1_before = W.ns_t1, t2_before = W.ns_t2;
+      const unsigned long long pushes_before = W.pushes;
       if (t.v[0] >= 0) {
         W.gid = t.graph;
         W.gp = graph_at(W, t.graph);
@@ -1623,6 +1786,8 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
         int nl = t.v[0] >= 0 ? W.gp->row_off[t.v[0] + 1] - W.gp->row_off[t.v[0]] : 0;
         max_info = ((unsigned long long)(unsigned)t.v[0] << 32) | (unsigned)nl;
         max_split = (W.ns_t1 - t1_before) / 1000 | ((W.ns_t2 - t2_before) / 1000 << 32);
+        max_pushes = W.pushes - pushes_before;
+        max_shape = t.v[0] >= 0 ? W.shape : 0;
         max_gid = W.gid;
       }
       if (lane == 0) {
@@ -1682,6 +1847,8 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
       // (counts-tier us) | (bitmap-tier us << 32), and the task's graph
       atomicExch(&ctl->max_task_split, (unsigned long long)max_split);
       atomicExch(&ctl->max_task_graph, (unsigned long long)max_gid);
+      atomicExch(&ctl->max_task_pushes, (unsigned long long)max_pushes);
+      atomicExch(&ctl->max_task_shape, (unsigned long long)max_shape);
     }
   }
   if (p.record_exit) {

@@ -21,8 +21,16 @@ __global__ void mbe_enum_kernel(const DevGraph* graphs, const long long* root_pr
                                 int32_t* scratch, unsigned long long* exit_ns);
 
 constexpr int kSlotWordsHost = 32768;  // int32 words per sub-problem slot (128 KiB)
+// Largest first-touch bitmap per warp (kEnumWarps of them fit the 227 KiB a block may use).
+constexpr int kSeenMaxWords = 3584;
+// Dynamic shared memory of a launch with layout sl.
+inline size_t enum_smem_bytes(const ScratchLayout& sl) {
+  return (size_t)sl.seen_words * sizeof(uint32_t) * kEnumWarps;
+}
 // |P|*|L| from which a child is shared out while many warps wait for work.
 constexpr int32_t kShareMinWorkDefault = 64;
+// P candidates per part of a root split into parts.
+constexpr int32_t kRangeChunkDefault = 64;
 
 // Per-warp scratch layout for the given capacities.
 ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS);

@@ -126,6 +126,7 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   if (capC >= (1 << 24))
     return set_error(MBE_ERR_CAPACITY, "graph too large for the no-allocation pool");
   ScratchLayout sl = make_layout(nV, capC, capL, capS);
+  sl.seen_words = 0;  // first touches by global atomics: this launch uses no dynamic shared memory
 
   // Pool partition: control block, split ring, per-block timing, hash keys,
   // then as many 16-warp blocks of per-warp scratch as fit.

@@ -148,6 +148,8 @@ int allocate(mbe_server* s) {
   s->blocks = s->prm.blocks > 0 ? std::min(s->prm.blocks, dev_sms * occ) : dev_sms * occ;
   const int warps = s->blocks * kEnumWarps;
   s->sl = make_layout(s->map_words, s->capC, s->capL, s->capS);
+  SCK(cudaFuncSetAttribute(mbe_enum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)enum_smem_bytes(s->sl)));
   const size_t scratch = (size_t)s->sl.words_per_warp * warps * sizeof(int32_t);
   SCK(cudaMalloc((void**)&s->d_scratch, scratch));
   // Every warp's count map starts all-zero; each task leaves it so.
@@ -190,6 +192,7 @@ int allocate(mbe_server* s) {
   ep.vertex_split = s->prm.split_mode == 1 ? 1 : 0;
   ep.root_split = s->prm.split_mode == 1 ? 0 : std::max(s->prm.root_split_size, 0);
   ep.share_min_work = s->prm.share_min_work > 0 ? s->prm.share_min_work : kShareMinWorkDefault;
+  apply_range_split(s->prm, &ep.range_work, &ep.range_chunk);
   ep.server = 1;
   ep.serve.sctl = s->d_sctl;
   ep.serve.arr_blk = s->d_arr_blk;
@@ -211,7 +214,7 @@ int launch(mbe_server* s) {
   pool.slots = s->d_slots;
   pool.bits = s->d_slot_bits;
   pool.nslot = s->nslot;
-  mbe_enum_kernel<<<s->blocks, kEnumThreads, 0, s->s_run>>>(
+  mbe_enum_kernel<<<s->blocks, kEnumThreads, enum_smem_bytes(s->sl), s->s_run>>>(
       reinterpret_cast<const DevGraph*>(s->d_arena), nullptr, nullptr, s->ep, s->sl, s->d_ctl,
       s->d_q_tasks, s->d_q_seq, pool, s->d_scratch, nullptr);
   SCK(cudaGetLastError());

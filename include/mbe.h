@@ -92,7 +92,7 @@ typedef struct mbe_params {
                            /*   0 = its children's bitmap sub-problems go to idle warps     */
                            /*   1 = GMBE's vertex-tuple child tasks (src/IterFinderGpu.cu:835-910) */
   int32_t direct_max_c;    /* a task with |L| <= bitmap_max_l goes straight to the bitmap  */
-                           /*   tier only while |C| <= this (0 = 4096); larger candidate   */
+                           /*   tier only while |C| <= this (0 = 16384); larger candidate  */
                            /*   sets go through the counts tier's sparse pushes            */
   int32_t root_split_size; /* split_mode 0: a root task (one vertex) with |P|*|L| above    */
                            /*   this is split into GMBE's vertex-tuple child tasks, so a   */
@@ -101,6 +101,12 @@ typedef struct mbe_params {
   int32_t share_min_work;  /* split_mode 0: while over an eighth of the warps wait for    */
                            /*   work, any child with |P|*|L| >= this is shared out, beyond */
                            /*   the split test's children (0 = default 64)                 */
+  int32_t range_split_work; /* split_mode 0: a maximal root with |P|*|C| above this is   */
+                           /*   split into parts of range_chunk P candidates; each part  */
+                           /*   redoes the root's set-up and pushes, at the first level, */
+                           /*   only the candidates whose id hashes to it (earlier parts */
+                           /*   act as Q).  <= 0 = never (default)                       */
+  int32_t range_chunk;     /* P candidates per part (0 = default 64)                     */
 } mbe_params;
 
 typedef struct mbe_result {
@@ -124,6 +130,10 @@ typedef struct mbe_result {
    * (the launch's graph index: descriptor order in a batch). */
   double max_task_tier1_ms, max_task_tier2_ms;
   int32_t max_task_graph, reserved;
+  /* The longest task's pushes in the counts and bitmap tiers, its |C| and,
+   * for a root split into parts, its part and the number of parts. */
+  uint64_t max_task_pushes1, max_task_pushes2;
+  int32_t max_task_cands, max_task_part, max_task_parts, reserved2;
 } mbe_result;
 
 /* Default parameters: bound_height 20, bound_size 1500, prune 1. */

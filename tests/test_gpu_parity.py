@@ -182,3 +182,21 @@ def test_slot_reuse_across_graphs_is_exact(gm):
     finally:
         for G, _ in graphs:
             G.free()
+
+
+@pytest.mark.parametrize("work,chunk", [(1, 2), (1, 64), (1 << 10, 8), (1 << 22, 0), (0, 0)])
+def test_root_parts_do_not_change_result(gm, work, chunk):
+    # A heavy root split into parts by a hash of the candidate id: each part
+    # pushes its own first-level candidates, earlier parts act as Q, later
+    # ones stay candidates of the children.  Any split gives the same set.
+    cases = [planted(300, 200, blocks=6, seed=3, bsize=14), hub_graph(1),
+             random_bipartite(24, 36, 0.85, 1), random_bipartite(120, 90, 0.08, 4)]
+    for ro, co, nU in cases:
+        want = oracle.gmbe(ro, co, nU)
+        for bitmap in (0, -1):  # bitmap tier from set-up, or counts tier only
+            r = run(gm, ro, co, nU, range_split_work=work, range_chunk=chunk,
+                    bitmap_max_l=bitmap)
+            assert r.status == 0
+            assert (r.count, r.set_hash) == (want.count, want.set_hash)
+            if work == 1 and chunk == 2:
+                assert r.tasks_split > 0
