@@ -59,7 +59,8 @@ class Params(C.Structure):
                 ("shard_count", C.c_int32), ("shard_index", C.c_int32),
                 ("split_mode", C.c_int32), ("direct_max_c", C.c_int32),
                 ("root_split_size", C.c_int32), ("share_min_work", C.c_int32),
-                ("range_split_work", C.c_int32), ("range_chunk", C.c_int32)]
+                ("range_split_work", C.c_int32), ("range_chunk", C.c_int32),
+                ("eager_share", C.c_int32)]
 
 
 class Result(C.Structure):

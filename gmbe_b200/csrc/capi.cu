@@ -168,7 +168,9 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   s.cadj = take(S);
   s.masks = take((int64_t)(kKMax + 1) * C);  // bitmap-tier records (K+1 words each)
   s.sub_v = take(2 * C);
-  s.bound2 = take(C);
+  s.tcls = take(C);
+  s.ckey = take(2 * C);
+  s.ent = take(S);
   s.lkey = take(2 * T2);
   s.lmask = take((T2 + 3) * kKMax);
   s.t2_rec = take(2 * (T2 + 3));
@@ -285,6 +287,7 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.root_split = prm.split_mode == 1 ? 0 : std::max(prm.root_split_size, 0);
   ep.share_min_work = prm.share_min_work > 0 ? prm.share_min_work : kShareMinWorkDefault;
   apply_range_split(prm, &ep.range_work, &ep.range_chunk);
+  ep.eager_share = eager_share_of(prm);
   ep.n_graphs = spec.n_graphs;
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;

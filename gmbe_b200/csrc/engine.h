@@ -82,6 +82,8 @@ int engine_status(Workspace& ws, const EnumCtl& ctl);
 void fill_profile(const EnumCtl& ctl, mbe_result* out);
 
 // Root splitting settings of a launch from the parameters.
+inline int32_t eager_share_of(const mbe_params& prm) { return prm.eager_share > 0 ? 1 : 0; }
+
 inline void apply_range_split(const mbe_params& prm, int32_t* work, int32_t* chunk) {
   *work = prm.split_mode == 1 ? 0 : std::max(prm.range_split_work, 0);
   *chunk = prm.range_chunk > 0 ? prm.range_chunk : kRangeChunkDefault;

@@ -81,7 +81,8 @@ struct ScratchLayout {
   int64_t map, touched, cv, ncnt, bound, coff, fill, sidx;
   int64_t lv, llevel, lp, aoff, stack, lsize;
   int64_t aadj, cadj;
-  int64_t masks, sub_v, bound2;
+  int64_t masks, sub_v, tcls;  // tcls: class of each touched candidate of a sparse push
+  int64_t ckey, ent;           // ckey: hash key per candidate (uint64); ent: packed entries
   int64_t lkey, lmask;  // lkey is uint64 (8-byte aligned offset)
   int64_t t2_rec, t2_n, t2_cur, t2_top, r_sum, r_cnt;  // bitmap-tier stack; t2_rec, r_sum uint64
   int64_t act, tlist;
@@ -149,6 +150,7 @@ struct EnumParams {
   int32_t share_min_work;     // |P|*|L| of a child shared out while many warps wait
   int32_t range_work;         // > 0: a root with |P|*|L| above this is split into parts
   int32_t range_chunk;        // P candidates per part
+  int32_t eager_share;        // 1: counts-tier children passing the split test always go
   int32_t server;             // 1: graphs arrive while the launch runs (ServeLink)
   ServeLink serve;
 };

@@ -238,9 +238,14 @@ __device__ __forceinline__ bool big_enough(const Warp& W, int nP, int nL) {
 // dense graphs, where a few dozen candidates can hold millions of
 // bicliques.  The floor (share_min_work) keeps the tiniest children, whose
 // copy would cost the exporting warp more than running them, at home.
-__device__ bool should_export(Warp& W, int nP, int nL) {
+// `eager`: a child that passes the split test goes even when no warp waits
+// (the counts tier's parents are the heaviest tasks of a launch and are
+// claimed first; their children, queued ahead of new roots, keep every warp
+// busy instead of lengthening the parent).
+__device__ bool should_export(Warp& W, int nP, int nL, bool eager = false) {
   if (nP < 2 || nL < 2) return false;
   const bool big = big_enough(W, nP, nL);
+  if (eager && big) return true;
   const int d = export_demand(W);
   return (d == 2 && (big || (long long)nP * nL >= W.p.share_min_work)) || (d == 1 && big);
 }
@@ -695,6 +700,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
   const int32_t* ncnt = W.A(W.sl.ncnt);
   const int32_t* bound = W.A(W.sl.bound);
   const int32_t* cv = W.A(W.sl.cv);
+  const uint64_t* ckey = W.A64(W.sl.ckey);
   int32_t* sidx = W.A(W.sl.sidx);
   int32_t* lp = W.A(W.sl.lp);
   uint64_t* lkey = W.A64(W.sl.lkey);
@@ -728,7 +734,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
     if (sel) {
       int s = nsub + __popc(bal & lanemask_lt());
       sidx[i] = s;
-      subkey[s] = W.gp->vkey[cv[i]];
+      subkey[s] = ckey[i];
     }
     nsub += __popc(bal);
     // candidates before x are Q
@@ -805,8 +811,13 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
     }
   }
   __syncwarp();
-  // child counts over the kept rows; tl = candidates met
-  int nt = 0;
+  // Child counts over the kept rows.  tl = candidates met (each once);
+  // ent = every (candidate, row) entry met, packed p << 7 | r (r < 128), so
+  // that the child's masks come from one linear pass instead of a second walk.
+  int32_t* ent = W.A(W.sl.ent);
+  int32_t* tcls = W.A(W.sl.tcls);
+  const uint64_t* ckey = W.A64(W.sl.ckey);
+  int nt = 0, ne = 0;
   flat_rows(
       n,
       [&](int r, int& beg, int& len) {
@@ -814,39 +825,46 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
         beg = aoff[l];
         len = aoff[l + 1] - beg;
       },
-      [&](bool valid, int, int pos) {
+      [&](bool valid, int r, int pos) {
         int p = valid ? aadj[pos] : -1;
         bool first = false;
         if (p >= 0) first = count_first(W, cc, p);
+        const unsigned lt = lanemask_lt();
         unsigned bal = __ballot_sync(kFull, first);
-        if (first) tl[nt + __popc(bal & lanemask_lt())] = p;
+        if (first) tl[nt + __popc(bal & lt)] = p;
         nt += __popc(bal);
+        unsigned be = __ballot_sync(kFull, p >= 0);
+        if (p >= 0) ent[ne + __popc(be & lt)] = (p << 7) | r;
+        ne += __popc(be);
       });
   counts_done(W, tl, nt);
-  // R of the child, maximality, and the child's candidates (Q part first)
+  // R of the child, maximality, and each touched candidate's class (0 none,
+  // 1 Q, 2 P).  Lane-local counters keep the iterations independent, so
+  // their loads overlap.
   bool ism = true;
   uint64_t sR = 0;
   unsigned long long nR = 0;
-  int nq = 0, np = 0, ncand = 0, nqc = 0;
-  for (int b0 = 0; b0 < nt; b0 += 32) {
-    int q = b0 + lane;
-    bool isC = false;
-    int p = 0;
-    if (q < nt) {
-      p = tl[q];
-      int c = cc[p];
-      if (c == kept) {
-        sR += W.gp->vkey[cv[p]];
-        ++nR;
-        if (p < x && bound[p] >= level) ism = false;
-      } else {
-        isC = bound[p] >= level;
-      }
+  int ncand = 0, nqc = 0;
+#pragma unroll 4
+  for (int q = lane; q < nt; q += 32) {
+    const int p = tl[q];
+    const int c = cc[p];
+    const int b = bound[p];
+    int cls = 0;
+    if (c == kept) {
+      sR += ckey[p];
+      ++nR;
+      if (p < x && b >= level) ism = false;
+    } else if (b >= level) {
+      cls = p < x ? 1 : 2;
+      ++ncand;
+      nqc += cls == 1;
     }
-    ncand += __popc(__ballot_sync(kFull, isC));
-    nqc += __popc(__ballot_sync(kFull, isC && p < x));
+    tcls[q] = cls;
   }
   ism = __all_sync(kFull, ism);
+  ncand = warp_sum(ncand);
+  nqc = warp_sum(nqc);
   sR = warp_sum(sR) + t.sRtask;
   nR = warp_sum(nR) + t.nRtask;
   if (ism) {
@@ -855,12 +873,13 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   } else {
     W.nonmax += 1;
   }
+  __syncwarp();
   if (ism && kept > 1 && ncand > 0) {
     // Destination: an export slot when idle warps want work and the child is
     // big enough by GMBE's split test, else this warp's scratch.
     const int K = words_k(n), RS = K + 1;
     int slot = -1;
-    if (ncand <= slot_cap(K) && should_export(W, ncand - nqc, n)) {
+    if (ncand <= slot_cap(K) && should_export(W, ncand - nqc, n, W.p.eager_share != 0)) {
       slot = lane == 0 ? slot_alloc(W) : 0;
       slot = __shfl_sync(kFull, slot, 0);
     }
@@ -873,40 +892,33 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
       for (int b = lane; b < n; b += 32) lk[b] = lkey[b];
     }
+    // child indices: Q from the front, P from the back
+    int nq = 0, np = 0;
     for (int b0 = 0; b0 < nt; b0 += 32) {
       int q = b0 + lane;
-      int p = q < nt ? tl[q] : 0;
-      bool isC = q < nt && cc[p] != kept && bound[p] >= level;
-      bool isQ = isC && p < x;
-      bool isP = isC && p > x;
-      unsigned bq = __ballot_sync(kFull, isQ);
-      unsigned bp = __ballot_sync(kFull, isP);
+      const int cls = q < nt ? tcls[q] : 0;
+      const int p = q < nt ? tl[q] : 0;
+      unsigned bq = __ballot_sync(kFull, cls == 1);
+      unsigned bp = __ballot_sync(kFull, cls == 2);
       int s = -1;
-      if (isQ) s = nq + __popc(bq & lanemask_lt());
-      if (isP) s = ncand - 1 - (np + __popc(bp & lanemask_lt()));
+      if (cls == 1) s = nq + __popc(bq & lanemask_lt());
+      if (cls == 2) s = ncand - 1 - (np + __popc(bp & lanemask_lt()));
       if (s >= 0) {
         sidx[p] = s;
-        subkey[s] = W.gp->vkey[cv[p]];
+        subkey[s] = ckey[p];
       }
       nq += __popc(bq);
       np += __popc(bp);
     }
     __syncwarp();
     init_records(rec, K, ncand);
-    flat_rows(
-        n,
-        [&](int r, int& beg, int& len) {
-          int l = lp[r];
-          beg = aoff[l];
-          len = aoff[l + 1] - beg;
-        },
-        [&](bool valid, int r, int pos) {
-          if (!valid) return;
-          int p = aadj[pos];
-          if (p < 0) return;
-          int si = sidx[p];
-          if (si >= 0) atomicOr(&rec[(size_t)si * RS + 1 + (r >> 5)], 1u << (r & 31));
-        });
+#pragma unroll 4
+    for (int e = lane; e < ne; e += 32) {
+      const int pk = ent[e];
+      const int si = sidx[pk >> 7];
+      const int r = pk & 127;
+      if (si >= 0) atomicOr(&rec[(size_t)si * RS + 1 + (r >> 5)], 1u << (r & 31));
+    }
     __syncwarp();
     if (slot >= 0) {
       if (lane == 0) {
@@ -921,8 +933,9 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   }
   __syncwarp();
   // state after finder_pop(x, level), then clear the child scratch
+#pragma unroll 4
   for (int q = lane; q < nt; q += 32) {
-    int p = tl[q];
+    const int p = tl[q];
     if (bound[p] >= level && p != x && cc[p] == ncnt[p]) bound[p] = level - 1;
     cc[p] = 0;
     sidx[p] = -1;
@@ -938,7 +951,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
   int32_t* bound = W.A(W.sl.bound);
   int32_t* stack = W.A(W.sl.stack);
   int32_t* lsize = W.A(W.sl.lsize);
-  const int32_t* cv = W.A(W.sl.cv);
+  const uint64_t* ckey = W.A64(W.sl.ckey);
   const int32_t* coff = W.A(W.sl.coff);
   const int32_t* cadj = W.A(W.sl.cadj);
   const int32_t* aadj = W.A(W.sl.aadj);
@@ -1010,7 +1023,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       unsigned long long nR = 0;
       for (int i = lane; i < t.nC; i += 32) {
         if (ncnt[i] == kept) {
-          sR += W.gp->vkey[cv[i]];
+          sR += ckey[i];
           ++nR;
           int b = bound[i];
           if (i < cur && b >= level) ism = false;
@@ -1540,6 +1553,10 @@ __device__ void run_task(Warp& W, const Task& t) {
       tier2(W, nL, nC, nq, nend, sR, nR);
     } else {
       // ---- tier 1: local adjacency ----
+      {
+        uint64_t* ckey = W.A64(W.sl.ckey);  // hash key per candidate, for the pushes
+        for (int i = lane; i < nC; i += 32) ckey[i] = g.vkey[cv[i]];
+      }
       int32_t* llevel = W.A(W.sl.llevel);
       int32_t* aadj = W.A(W.sl.aadj);
       int32_t* coff = W.A(W.sl.coff);

@@ -107,6 +107,9 @@ typedef struct mbe_params {
                            /*   only the candidates whose id hashes to it (earlier parts */
                            /*   act as Q).  <= 0 = never (default)                       */
   int32_t range_chunk;     /* P candidates per part (0 = default 64)                     */
+  int32_t eager_share;     /* split_mode 0: a child of the counts tier (|L| > bitmap_max_l) */
+                           /*   that passes the split test is shared out even while no  */
+                           /*   warp waits: 1 = yes, <= 0 = no (default)                */
 } mbe_params;
 
 typedef struct mbe_result {
