@@ -35,6 +35,12 @@ UNIT = "bicliques/s"
 FLAGS = dict(uvtrans=1, order=1, fast_mode=1)
 CONSTS = os.path.join(ROOT, "gmbe_b200", "workload_constants.json")
 FALLBACK_HBM_GBS = 6650.0
+_T0 = time.time()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
 def load_consts():
@@ -189,7 +195,9 @@ def batched_leg(n=4096, replays=3, plain_stride=4):
     launch per graph on every plain_stride-th graph (graphs resident on the
     device in both arms); per-graph results must be equal."""
     import gmbe_b200 as gm
+    log("batched: generating")
     gs = [gm.batch_graph(1000 + i) for i in range(n)]
+    log("batched: building")
     B = gm.Batch(gs)
     per, tot = B.run()  # capture + warm-up
     walls = []
@@ -198,6 +206,7 @@ def batched_leg(n=4096, replays=3, plain_stride=4):
         per, tot = B.run()
         walls.append(time.perf_counter() - t)
     wall = statistics.median(walls)
+    log("batched: plain arm")
     sample = list(range(0, n, plain_stride))
     Gs = [gm.Graph.from_csr(gs[i].row_off, gs[i].col, gs[i].nU, **FLAGS) for i in sample]
     Gs[0].enumerate()
@@ -227,16 +236,19 @@ def serving_leg(n=1000, rates=(1000, 5000, 20000)):
     import numpy as np
     import gmbe_b200 as gm
     from gmbe_b200.configs import serve_mix
+    log("serving: generating")
     reqs, is_med = serve_mix(n)
     rng = np.random.default_rng(7)
     pct = lambda x, q: float(np.percentile(x, q)) * 1e3
     srv = gm.Server(max_v=32768, max_degree=4096, max_two_hop=1 << 17, arena_bytes=8 << 30,
                     max_graphs=4096)
+    log("serving: warm-up")
     for g in reqs[:20]:
-        srv.wait(srv.submit(g.row_off, g.col, g.nU), timeout=300)
+        srv.wait(srv.submit(g.row_off, g.col, g.nU), timeout=60)
     loads, outs = {}, []
     arrivals = {}
     for rate in rates:
+        log(f"serving: offered load {rate}/s")
         arr = np.cumsum(rng.exponential(1.0 / rate, n))
         arrivals[rate] = arr
         t0 = time.perf_counter()
@@ -247,7 +259,7 @@ def serving_leg(n=1000, rates=(1000, 5000, 20000)):
             sub.append((srv.submit(g.row_off, g.col, g.nU), time.perf_counter() - t0))
         lat, fin, out = [], [], []
         for (rid, ts), a in zip(sub, arr):
-            r = srv.wait(rid, timeout=600)
+            r = srv.wait(rid, timeout=120)
             out.append((r.count, r.set_hash))
             lat.append(ts + r.enum_seconds - a)
             fin.append(ts + r.enum_seconds)
@@ -256,6 +268,7 @@ def serving_leg(n=1000, rates=(1000, 5000, 20000)):
                             "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
     st = srv.stats()
     srv.close()
+    log("serving: plain arm")
     svc, plain = [], []
     for g in reqs:
         t = time.perf_counter()
@@ -373,6 +386,7 @@ def main():
     value = consts["count"] * args.steps / (total_ms / 1000.0)
 
     # ---- end to end through the public API with host buffers ----
+    log("timed steps done; end-to-end calls")
     e2e_steps = max(1, min(args.steps, 3))
     # CSR, its transpose and the per-vertex hash keys are uploaded per call.
     h2d = 4 * ((g.nV + 1) + (g.nU + 1) + 2 * g.nE) + 8 * (g.nV + g.nU)
@@ -420,6 +434,7 @@ def main():
             line["batched"] = batched_leg()
             line["serving"] = serving_leg()
         if world == 1 and not args.no_cpu_baseline:
+            log("CPU baseline")
             v, sample, cores = cpu_sample(g)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                                     "sample": sample}

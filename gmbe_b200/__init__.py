@@ -101,7 +101,10 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
                 ("rejected", C.c_uint64), ("cancelled", C.c_uint64), ("launches", C.c_uint64),
                 ("arena_resets", C.c_uint64), ("resident", C.c_int64), ("waiting", C.c_int64),
-                ("arena_used", C.c_int64), ("arena_bytes", C.c_int64)]
+                ("arena_used", C.c_int64), ("arena_bytes", C.c_int64),
+                ("published", C.c_uint64), ("collected", C.c_uint64),
+                ("launch_running", C.c_int64), ("dev_head", C.c_uint64), ("dev_tail", C.c_uint64),
+                ("dev_done", C.c_uint64), ("dev_pending", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -145,6 +148,7 @@ _sig = {
     "mbe_server_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
     "mbe_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "mbe_server_destroy": (C.c_int, [C.c_void_p]),
+    "mbe_server_debug_request": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(_lib, _name)
@@ -346,6 +350,12 @@ class Server:
         st = ServerStats()
         _check(_lib.mbe_server_get_stats(self._h, C.byref(st)))
         return st.as_dict()
+
+    def debug_request(self, rid: int) -> dict:
+        """A resident request's device counters (diagnosis)."""
+        out = (C.c_uint64 * 4)()
+        _check(_lib.mbe_server_debug_request(self._h, rid, out))
+        return dict(roots_claimed=out[0], pending=out[1], n_roots=out[2], block=out[3])
 
     def close(self):
         if self._h and self._h.value:

@@ -582,32 +582,48 @@ __device__ void tier2(Warp& W, int n, int nsub, int nq, int nend, uint64_t sR0, 
 }
 
 // Runs an exported sub-problem and releases its slot.  The slot was written
-// by another warp, possibly on another SM, and may have been read here
-// before under an older owner: every lane fences before its first read.
-// The run writes bounds into the slot's level-0 records, so every lane
-// fences again before the slot is freed; without that a store still in
-// flight could land on the records of the slot's next owner.
+// by another warp, possibly on another SM, and this SM may hold lines of it
+// from an older owner in its (non-coherent) L1: the header is read with
+// volatile loads and the body is copied through L2 (ld.global.cg) into this
+// warp's own scratch, where the sub-problem then runs.  The slot is freed as
+// soon as it is copied; nothing here writes it, so no store can land on the
+// records of its next owner.
 __device__ void tier2_from_slot(Warp& W, int slot) {
-  __threadfence();
+  const int lane = (int)lane_id();
   int32_t* sp = W.slots + (size_t)slot * kSlotWords;
+  volatile const int32_t* vh = sp;
+  const int K = vh[0];
+  const int nsub = vh[1];
+  const int nq = vh[2];
+  const int32_t gid = vh[3];
   T2Src src;
-  const int K = sp[0];
-  src.nsub = sp[1];
-  src.nq = sp[2];
-  src.nend = src.nsub;
-  W.gid = sp[3];
-  W.gp = graph_at(W, W.gid);
-  for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)sp[4 + w];
-  src.sR0 = *reinterpret_cast<const uint64_t*>(sp + 8);
-  src.nR0 = (uint32_t)sp[10];
-  src.lkey = reinterpret_cast<const uint64_t*>(sp + kSlotLkey);
-  src.rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
-  src.subkey = slot_subkey(sp, K, src.nsub);
+  for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)vh[4 + w];
+  src.sR0 = (uint64_t)(uint32_t)vh[8] | ((uint64_t)(uint32_t)vh[9] << 32);
+  src.nR0 = (uint32_t)vh[10];
+  const int RS = K + 1;
+  uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
+  uint64_t* subkey = W.A64(W.sl.sub_v);
+  uint64_t* lkey = W.A64(W.sl.lkey);
+  const unsigned* srec = reinterpret_cast<const unsigned*>(sp + kSlotRec);
+  const unsigned long long* skey =
+      reinterpret_cast<const unsigned long long*>(slot_subkey(sp, K, nsub));
+  const unsigned long long* slk = reinterpret_cast<const unsigned long long*>(sp + kSlotLkey);
+  const int nw = nsub * RS;
+  for (int i = lane; i < nw; i += 32) rec[i] = __ldcg(srec + i);
+  for (int i = lane; i < nsub; i += 32) subkey[i] = __ldcg(skey + i);
+  for (int i = lane; i < 32 * K; i += 32) lkey[i] = __ldcg(slk + i);
+  __syncwarp();
+  if (lane == 0) slot_free(W, slot);
+  __syncwarp();
+  W.gid = gid;
+  W.gp = graph_at(W, gid);
+  src.rec = rec;
+  src.subkey = subkey;
+  src.lkey = lkey;
+  src.nsub = nsub;
+  src.nq = nq;
+  src.nend = nsub;
   tier2_dispatch(W, src, K);
-  __threadfence();
-  __syncwarp();
-  if (lane_id() == 0) slot_free(W, slot);
-  __syncwarp();
 }
 
 // Zeroes nsub records of K+1 words, each with its index and a free bound.

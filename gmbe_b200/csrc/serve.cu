@@ -52,6 +52,7 @@ struct Request {
   std::vector<char> image;  // the arena block; descriptor pointers patched on admission
   size_t bytes = 0;         // image size, a multiple of kBlock
   size_t o_row_off = 0, o_col = 0, o_rev_off = 0, o_rev_col = 0, o_ukey = 0, o_vkey = 0;
+  size_t arena_off = 0;  // where it was placed, once admitted
   DevGraph dg;
   double t_submit = 0;
   mbe_result res;
@@ -85,7 +86,7 @@ struct mbe_server {
   ScratchLayout sl;
   EnumParams ep;
   int32_t capC = 1, capL = 1, capS = 1, map_words = 1;
-  cudaStream_t s_run = nullptr, s_copy = nullptr;
+  cudaStream_t s_run = nullptr, s_copy = nullptr, s_peek = nullptr;
   cudaEvent_t ev_run = nullptr, ev_copy = nullptr;
   bool running = false;
   // Host side, under mu.
@@ -130,6 +131,7 @@ void release(mbe_server* s) {
   if (s->ev_copy) cudaEventDestroy(s->ev_copy);
   if (s->s_run) cudaStreamDestroy(s->s_run);
   if (s->s_copy) cudaStreamDestroy(s->s_copy);
+  if (s->s_peek) cudaStreamDestroy(s->s_peek);
   for (auto& kv : s->reqs) delete kv.second;
   s->reqs.clear();
 }
@@ -179,6 +181,7 @@ int allocate(mbe_server* s) {
   }
   SCK(cudaStreamCreateWithFlags(&s->s_run, cudaStreamNonBlocking));
   SCK(cudaStreamCreateWithFlags(&s->s_copy, cudaStreamNonBlocking));
+  SCK(cudaStreamCreateWithFlags(&s->s_peek, cudaStreamNonBlocking));
   SCK(cudaEventCreateWithFlags(&s->ev_run, cudaEventDisableTiming));
   SCK(cudaEventCreateWithFlags(&s->ev_copy, cudaEventDisableTiming));
   SCK(cudaDeviceSynchronize());
@@ -270,6 +273,7 @@ int admit(mbe_server* s, Request* r) {
   SCK(cudaMemcpyAsync(&s->d_sctl->arr_tail, &tail, sizeof(tail), cudaMemcpyHostToDevice,
                       s->s_copy));
   SCK(cudaEventRecord(s->ev_copy, s->s_copy));
+  r->arena_off = off;
   s->bump = off + r->bytes;
   s->published++;
   s->resident++;
@@ -570,6 +574,42 @@ int mbe_server_get_stats(mbe_server* s, mbe_server_stats* out) {
   out->waiting = (int64_t)s->waiting.size();
   out->arena_used = (int64_t)s->bump;
   out->arena_bytes = s->cfg.arena_bytes;
+  out->published = s->published;
+  out->collected = s->collected;
+  out->launch_running = s->running ? 1 : 0;
+  // Device side, read on a stream of its own while a launch may run.
+  ServeCtl sc;
+  EnumCtl ctl;
+  cudaSetDevice(s->device);
+  if (cudaMemcpyAsync(&sc, s->d_sctl, sizeof(sc), cudaMemcpyDeviceToHost, s->s_peek) == cudaSuccess &&
+      cudaMemcpyAsync(&ctl, s->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s->s_peek) == cudaSuccess &&
+      cudaStreamSynchronize(s->s_peek) == cudaSuccess) {
+    out->dev_head = sc.arr_head;
+    out->dev_tail = sc.arr_tail;
+    out->dev_done = sc.done_pos;
+    out->dev_pending = ctl.pending;
+  }
+  return MBE_OK;
+}
+
+int mbe_server_debug_request(mbe_server* s, uint64_t request_id, uint64_t out[4]) {
+  clear_error();
+  if (!s || !out) return set_error(MBE_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(request_id);
+  if (it == s->reqs.end() || it->second->state != kResident)
+    return set_error(MBE_ERR_INVALID, "request %llu is not on the device",
+                     (unsigned long long)request_id);
+  ServeGraph hdr;
+  cudaSetDevice(s->device);
+  if (cudaMemcpyAsync(&hdr, s->d_arena + it->second->arena_off, sizeof(hdr),
+                      cudaMemcpyDeviceToHost, s->s_peek) != cudaSuccess ||
+      cudaStreamSynchronize(s->s_peek) != cudaSuccess)
+    return set_error(MBE_ERR_CUDA, "reading the request's block failed");
+  out[0] = hdr.next_root;
+  out[1] = hdr.pending;
+  out[2] = (uint64_t)hdr.g.n_roots;
+  out[3] = it->second->arena_off >> kServeBlockShift;
   return MBE_OK;
 }
 

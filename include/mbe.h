@@ -283,6 +283,12 @@ typedef struct mbe_server_stats {
   int64_t resident;       /* admitted, not yet finished */
   int64_t waiting;        /* submitted, not yet admitted */
   int64_t arena_used, arena_bytes;
+  /* Progress, for diagnosis: graphs published to the device and completions
+   * collected; whether a launch runs; the device's arrival head and tail,
+   * completions handed out, and tasks in flight in the current launch. */
+  uint64_t published, collected;
+  int64_t launch_running;
+  uint64_t dev_head, dev_tail, dev_done, dev_pending;
 } mbe_server_stats;
 
 void mbe_server_config_default(mbe_server_config* c);
@@ -312,6 +318,11 @@ int mbe_server_wait(mbe_server* s, uint64_t request_id, int64_t timeout_ns, mbe_
 int mbe_server_cancel(mbe_server* s, uint64_t request_id);
 
 int mbe_server_get_stats(mbe_server* s, mbe_server_stats* out);
+
+/* Diagnosis: a resident request's device counters -- roots claimed, tasks
+ * outstanding, roots in all, and its arena block (out[0..3]).
+ * MBE_ERR_INVALID if the request is not on the device. */
+int mbe_server_debug_request(mbe_server* s, uint64_t request_id, uint64_t out[4]);
 
 /* Stops the launch (graphs still on the GPU are abandoned) and frees all. */
 int mbe_server_destroy(mbe_server* s);
