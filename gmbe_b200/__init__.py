@@ -125,6 +125,7 @@ _sig = {
                                    _P32, _P32, C.POINTER(C.c_int64)]),
     "mbe_gen_batch_spec": (C.c_int, [C.c_uint64, C.POINTER(GenSpec)]),
     "mbe_write_adj": (C.c_int, [C.c_char_p, _P32, _P32, C.c_int32]),
+    "mbe_write_graph": (C.c_int, [C.c_char_p, _P32, _P32, C.c_int32]),
     "mbe_read_adj": (C.c_int, [C.c_char_p, C.POINTER(_P32), C.POINTER(_P32), _P32, _P32,
                                C.POINTER(C.c_int64)]),
     "mbe_free": (None, [C.c_void_p]),
@@ -417,6 +418,12 @@ def batch_spec(seed: int) -> GenSpec:
 def write_adj(path: str, g: BipartiteCSR):
     ro, co = _i32(g.row_off), _i32(g.col)
     _check(_lib.mbe_write_adj(os.fsencode(path), _ptr(ro), _ptr(co), g.nV))
+
+
+def write_graph(path: str, g: BipartiteCSR):
+    """Edge-pair .graph file for the CPU peers (mbe_write_graph)."""
+    ro, co = _i32(g.row_off), _i32(g.col)
+    _check(_lib.mbe_write_graph(os.fsencode(path), _ptr(ro), _ptr(co), g.nV))
 
 
 def read_adj(path: str) -> BipartiteCSR:

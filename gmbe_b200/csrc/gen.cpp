@@ -252,6 +252,22 @@ extern "C" int mbe_write_adj(const char* path, const int32_t* row_off, const int
   return MBE_OK;
 }
 
+extern "C" int mbe_write_graph(const char* path, const int32_t* row_off, const int32_t* col,
+                               int32_t nV) {
+  clear_error();
+  if (!path || (nV > 0 && (!row_off || !col))) return set_error(MBE_ERR_INVALID, "null argument");
+  int32_t umax = -1;
+  for (int64_t i = 0; nV > 0 && i < (int64_t)row_off[nV]; ++i) umax = std::max(umax, col[i]);
+  FILE* fp = fopen(path, "wb");
+  if (!fp) return set_error(MBE_ERR_IO, "cannot write %s", path);
+  bool ok = fprintf(fp, "%d %d\n", nV, umax + 1) > 0;
+  for (int32_t v = 0; ok && v < nV; ++v)
+    for (int32_t i = row_off[v]; ok && i < row_off[v + 1]; ++i)
+      ok = fprintf(fp, "%d %d\n", v, col[i]) > 0;
+  if (fclose(fp) != 0) ok = false;
+  return ok ? MBE_OK : set_error(MBE_ERR_IO, "short write to %s", path);
+}
+
 extern "C" int mbe_read_adj(const char* path, int32_t** row_off_out, int32_t** col_out,
                             int32_t* nV, int32_t* nU, int64_t* nE) {
   clear_error();

@@ -366,6 +366,11 @@ int mbe_gen_batch_spec(uint64_t seed, mbe_gen_spec* out);
 /* Write an .adj file (one line per V row, space-separated ascending U ids). */
 int mbe_write_adj(const char* path, const int32_t* row_off, const int32_t* col, int32_t nV);
 
+/* Write the edge-pair .graph form read by the CPU peers (PARMBE, ooMBEA):
+ * a first line "<rows> <max id + 1>", then one line "<row> <id>" per entry
+ * in row order (replaces preprocess/adj_to_graph.cpp). */
+int mbe_write_graph(const char* path, const int32_t* row_off, const int32_t* col, int32_t nV);
+
 /* Parse an .adj file into library-owned host arrays without uploading. */
 int mbe_read_adj(const char* path, int32_t** row_off, int32_t** col, int32_t* nV, int32_t* nU,
                  int64_t* nE);

@@ -253,3 +253,24 @@ def test_server_needs_a_device(gm):
     with pytest.raises(gm.MBEError) as ei:
         gm.Server()
     assert ei.value.name == "MBE_ERR_CUDA"
+
+
+def test_graph_writer_matches_reference_converter(gm, tmp_path):
+    # The edge-pair .graph file the CPU peers read.  Where the reference's own
+    # converter (preprocess/adj_to_graph.cpp) is built into oracle/_ref, both
+    # files must be identical byte for byte; otherwise the format is checked.
+    ro, co, nU = planted(60, 40, blocks=2, seed=21)
+    g = gm.BipartiteCSR(ro, co, nU)
+    adj, ours = tmp_path / "g.adj", tmp_path / "ours.graph"
+    gm.write_adj(str(adj), g)
+    gm.write_graph(str(ours), g)
+    lines = ours.read_text().splitlines()
+    assert lines[0] == f"{g.nV} {int(co.max()) + 1}"
+    pairs = [tuple(map(int, l.split())) for l in lines[1:]]
+    want = [(v, int(u)) for v in range(g.nV) for u in co[ro[v]:ro[v + 1]]]
+    assert pairs == want
+    conv = oracle.ref_binary("adj_to_graph")
+    if conv:
+        theirs = tmp_path / "theirs.graph"
+        subprocess.run([conv, str(adj), str(theirs)], check=True, capture_output=True)
+        assert ours.read_bytes() == theirs.read_bytes()
