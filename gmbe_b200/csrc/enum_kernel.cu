@@ -245,9 +245,11 @@ __device__ __forceinline__ bool big_enough(const Warp& W, int nP, int nL) {
 __device__ bool should_export(Warp& W, int nP, int nL, bool eager = false) {
   if (nP < 2 || nL < 2) return false;
   const bool big = big_enough(W, nP, nL);
+  const bool sizable = (long long)nP * nL >= W.p.share_min_work;
+  if (!big && !sizable) return false;  // goes at no demand: skip reading it
   if (eager && big) return true;
   const int d = export_demand(W);
-  return (d == 2 && (big || (long long)nP * nL >= W.p.share_min_work)) || (d == 1 && big);
+  return (d == 2 && (big || sizable)) || (d == 1 && big);
 }
 
 // Enqueues a filled slot as a task; false if the ring is full.
