@@ -120,6 +120,8 @@ _sig = {
     "mbe_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(GraphInfo)]),
     "mbe_graph_free": (C.c_int, [C.c_void_p]),
     "mbe_enumerate": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]),
+    "mbe_enumerate_emit": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result), _P32,
+                                     C.c_int64, C.POINTER(C.c_int64)]),
     "mbe_last_error_string": (C.c_char_p, []),
     "mbe_gen_chung_lu": (C.c_int, [C.POINTER(GenSpec), C.POINTER(_P32), C.POINTER(_P32),
                                    _P32, _P32, C.POINTER(C.c_int64)]),
@@ -222,6 +224,23 @@ class Graph:
         r = Result()
         _check(_lib.mbe_enumerate(self._h, C.byref(p), C.byref(r)))
         return r
+
+    def enumerate_emit(self, buf_words: int = 1 << 22, **params):
+        """mbe_enumerate_emit: (Result, [(U ids, V ids), ...]) in original ids."""
+        p = default_params(**params)
+        r = Result()
+        buf = np.zeros(max(buf_words, 2), np.int32)
+        used = C.c_int64()
+        _check(_lib.mbe_enumerate_emit(self._h, C.byref(p), C.byref(r), _ptr(buf), buf_words,
+                                       C.byref(used)))
+        out, pos, n = [], 0, used.value
+        while pos < n:
+            nu, nv = int(buf[pos]), int(buf[pos + 1])
+            us = tuple(int(x) for x in buf[pos + 2:pos + 2 + nu])
+            vs = tuple(int(x) for x in buf[pos + 2 + nu:pos + 2 + nu + nv])
+            out.append((us, vs))
+            pos += 2 + nu + nv
+        return r, out
 
     def free(self):
         if self._h and self._h.value:

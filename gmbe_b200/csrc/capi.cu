@@ -4,6 +4,7 @@
 #include <sys/time.h>
 
 #include <algorithm>
+#include <iterator>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -172,6 +173,7 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   s.ckey = take(2 * C);
   s.ent = take(S);
   s.lkey = take(2 * T2);
+  s.lid = take(T2);
   s.lmask = take((T2 + 3) * kKMax);
   s.t2_rec = take(2 * (T2 + 3));
   s.t2_n = take(T2 + 3);
@@ -436,7 +438,10 @@ int mbe_graph_free(mbe_graph* g) {
   return MBE_OK;
 }
 
-int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
+// mbe_enumerate, optionally writing biclique records into d_emit (emit_cap
+// words) and reporting the words reserved in *emit_pos.
+static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* out,
+                           int32_t* d_emit, long long emit_cap, unsigned long long* emit_pos) {
   clear_error();
   if (!g || !out) return set_error(MBE_ERR_INVALID, "null argument");
   memset(out, 0, sizeof(*out));
@@ -486,6 +491,8 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   spec.n_graphs = 1;
   LaunchPlan plan;
   if ((rc = engine_prepare(ws, spec, prm, &plan))) return rc;
+  plan.ep.emit = d_emit;
+  plan.ep.emit_cap = emit_cap;
   long long prefix[2] = {0, n_roots};
   CK(cudaMemcpyAsync(ws.d_graph1, &dg, sizeof(dg), cudaMemcpyHostToDevice, 0));
   CK(cudaMemcpyAsync(ws.d_prefix1, prefix, sizeof(prefix), cudaMemcpyHostToDevice, 0));
@@ -515,7 +522,84 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
     out->warp_busy_frac = ms > 0 ? busy / 1e6 / ((double)plan.warps * ms) : 0.0;
   }
   out->enum_seconds = now_s() - t0;
+  if (emit_pos) *emit_pos = ctl.emit_pos;
   return engine_status(ws, ctl);
+}
+
+int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
+  return enumerate_graph(g, params, out, nullptr, 0, nullptr);
+}
+
+int mbe_enumerate_emit(mbe_graph* g, const mbe_params* params, mbe_result* out, int32_t* buf,
+                       int64_t buf_words, int64_t* used_words) {
+  clear_error();
+  if (!g || !out || !used_words || buf_words < 0 || (buf_words > 0 && !buf))
+    return set_error(MBE_ERR_INVALID, "null or negative argument");
+  *used_words = 0;
+  CK(cudaSetDevice(g->device));
+  // Device records ([|L|, graph, L]) are never longer than the output records
+  // ([|U|, |V|, U, V]) they become, so a device buffer of buf_words suffices.
+  const long long dcap = std::max<long long>(buf_words, 2);
+  int32_t* d_emit = nullptr;
+  CK(cudaMalloc((void**)&d_emit, sizeof(int32_t) * (size_t)dcap));
+  int rc = MBE_OK;
+  unsigned long long reserved = 0;
+  std::vector<int32_t> dev;
+  cudaError_t e = cudaMemset(d_emit, 0, sizeof(int32_t) * (size_t)dcap);
+  if (e != cudaSuccess) rc = set_error(MBE_ERR_CUDA, "clearing the record buffer: %s", cudaGetErrorString(e));
+  if (!rc) rc = enumerate_graph(g, params, out, d_emit, dcap, &reserved);
+  if (!rc) {
+    dev.resize((size_t)std::min<unsigned long long>(reserved, (unsigned long long)dcap));
+    e = cudaMemcpy(dev.data(), d_emit, sizeof(int32_t) * dev.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = set_error(MBE_ERR_CUDA, "reading the records: %s", cudaGetErrorString(e));
+  }
+  cudaFree(d_emit);
+  if (rc) return rc;
+  // Records: R = N(L) from the internal U -> V lists; both sides to original
+  // ids (internal U is the original V side when -t swapped them).
+  const HostGraph& h = g->h;
+  std::vector<int32_t> L, R, tmp, us, vs;
+  size_t pos = 0;
+  int64_t used = 0;
+  bool full = false;
+  while (pos + 2 <= dev.size() && dev[pos] > 0) {
+    const int32_t nl = dev[pos];
+    if (pos + 2 + (size_t)nl > dev.size()) break;
+    L.assign(dev.begin() + pos + 2, dev.begin() + pos + 2 + nl);
+    pos += 2 + (size_t)nl;
+    int32_t best = L[0];
+    for (int32_t u : L)
+      if (h.rev_off[u + 1] - h.rev_off[u] < h.rev_off[best + 1] - h.rev_off[best]) best = u;
+    R.assign(h.rev_col.begin() + h.rev_off[best], h.rev_col.begin() + h.rev_off[best + 1]);
+    for (int32_t u : L) {
+      if (u == best) continue;
+      tmp.clear();
+      std::set_intersection(R.begin(), R.end(), h.rev_col.begin() + h.rev_off[u],
+                            h.rev_col.begin() + h.rev_off[u + 1], std::back_inserter(tmp));
+      R.swap(tmp);
+    }
+    us.clear();
+    vs.clear();
+    for (int32_t u : L) (h.swapped ? vs : us).push_back(h.u_orig[u]);
+    for (int32_t v : R) (h.swapped ? us : vs).push_back(h.v_orig[v]);
+    std::sort(us.begin(), us.end());
+    std::sort(vs.begin(), vs.end());
+    const int64_t need = 2 + (int64_t)us.size() + (int64_t)vs.size();
+    if (used + need > buf_words) {
+      full = true;
+      break;
+    }
+    buf[used] = (int32_t)us.size();
+    buf[used + 1] = (int32_t)vs.size();
+    std::copy(us.begin(), us.end(), buf + used + 2);
+    std::copy(vs.begin(), vs.end(), buf + used + 2 + us.size());
+    used += need;
+  }
+  *used_words = used;
+  if (full || reserved > (unsigned long long)dcap)
+    return set_error(MBE_ERR_CAPACITY, "record buffer of %lld words too small (%llu device words reserved)",
+                     (long long)buf_words, reserved);
+  return MBE_OK;
 }
 
 }  // extern "C"

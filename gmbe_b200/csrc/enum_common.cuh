@@ -70,6 +70,7 @@ struct EnumCtl {
   unsigned long long max_task_pushes; // its pushes: counts tier | bitmap tier << 32
   unsigned long long max_task_shape;  // its |C| | part << 32 | parts << 48 (root tasks)
   unsigned long long n_tasks, n_tier2;
+  unsigned long long emit_pos;  // words of biclique records reserved (may pass the buffer's end)
 };
 
 // Per-warp scratch layout (int32 words unless noted), offsets in words from
@@ -84,6 +85,7 @@ struct ScratchLayout {
   int64_t masks, sub_v, tcls;  // tcls: class of each touched candidate of a sparse push
   int64_t ckey, ent;           // ckey: hash key per candidate (uint64); ent: packed entries
   int64_t lkey, lmask;  // lkey is uint64 (8-byte aligned offset)
+  int64_t lid;          // internal U id of each bitmap-tier L bit (for emission)
   int64_t t2_rec, t2_n, t2_cur, t2_top, r_sum, r_cnt;  // bitmap-tier stack; t2_rec, r_sum uint64
   int64_t act, tlist;
   int32_t act_cap;
@@ -151,6 +153,8 @@ struct EnumParams {
   int32_t range_work;         // > 0: a root with |P|*|L| above this is split into parts
   int32_t range_chunk;        // P candidates per part
   int32_t eager_share;        // 1: counts-tier children passing the split test always go
+  int32_t* emit;              // biclique records [|L|, graph, L ids...], or null
+  long long emit_cap;         // words in emit
   int32_t server;             // 1: graphs arrive while the launch runs (ServeLink)
   ServeLink serve;
 };

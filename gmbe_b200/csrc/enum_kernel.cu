@@ -124,6 +124,36 @@ __device__ __forceinline__ void counts_done(const Warp& W, const int32_t* idx, i
   }
 }
 
+// Emission (opt-in): appends a maximal biclique's L to the launch's record
+// buffer as [|L|, graph, internal U ids of L...]; R is N(L).  The L members
+// are the positions l < nscan with sel(l), `count` of them, id(l) each.  A
+// record that does not fit entirely is dropped (the reserved word count keeps
+// growing past the buffer, which tells the host).  The host zeroes the buffer
+// first, so a zero length word marks the end of what was written.
+template <typename Sel, typename Id>
+__device__ void emit_biclique(const Warp& W, int count, int nscan, Sel sel, Id id) {
+  int32_t* buf = W.p.emit;
+  if (!buf) return;
+  const int lane = (int)lane_id();
+  unsigned long long pos = 0;
+  if (lane == 0) pos = atomicAdd(&W.ctl->emit_pos, (unsigned long long)count + 2);
+  pos = __shfl_sync(kFull, pos, 0);
+  if (pos + (unsigned long long)count + 2 > (unsigned long long)W.p.emit_cap) return;
+  int out = 0;
+  for (int b0 = 0; b0 < nscan; b0 += 32) {
+    const int l = b0 + lane;
+    const bool s = l < nscan && sel(l);
+    const unsigned bal = __ballot_sync(kFull, s);
+    if (s) buf[pos + 2 + out + __popc(bal & lanemask_lt())] = id(l);
+    out += __popc(bal);
+  }
+  if (lane == 0) {
+    buf[pos + 1] = W.gid;
+    buf[pos] = count;
+  }
+  __syncwarp();
+}
+
 // Serving block of graph `gid` (a block index into the arena, which the
 // launch receives in place of the descriptor array).
 __device__ __forceinline__ ServeGraph* serve_graph(const Warp& W, int32_t gid) {
@@ -167,6 +197,7 @@ struct T2Src {
   uint32_t* rec;           // nsub records, writable (their bounds change)
   const uint64_t* subkey;
   const uint64_t* lkey;
+  const int32_t* lid;      // internal U id of each L bit (emission only)
   uint32_t L0[4];          // the sub-problem's L
   int nsub, nq;            // records [0, nq) are Q, [nq, nsub) P
   int nend;                // the first level pushes records [nq, nend) only
@@ -178,7 +209,8 @@ struct T2Src {
 constexpr int kSlotWords = 32768;
 constexpr int kSlotHdr = 16;
 constexpr int kSlotLkey = kSlotHdr;
-constexpr int kSlotRec = kSlotLkey + 2 * 32 * 4;
+constexpr int kSlotLid = kSlotLkey + 2 * 32 * 4;  // 128 int32: the L bits' vertex ids
+constexpr int kSlotRec = kSlotLid + 32 * 4;
 __host__ __device__ constexpr int slot_cap(int K) {
   return ((kSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
 }
@@ -297,7 +329,11 @@ __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, 
     for (int w = 0; w < K; ++w) rec[(size_t)q * RS + 1 + w] = c[1 + w];
     key[q] = src.subkey[c[0] >> 8];
   }
-  for (int b = lane; b < 32 * K; b += 32) lk[b] = src.lkey[b];
+  int32_t* li = sp + kSlotLid;
+  for (int b = lane; b < 32 * K; b += 32) {
+    lk[b] = src.lkey[b];
+    li[b] = src.lid[b];
+  }
   if (lane == 0) slot_header(sp, K, nchild, nbefore, Ln, sR, nR, W.gid);
   if (slot_publish(W, slot)) return true;
   if (lane == 0) slot_free(W, slot);
@@ -461,6 +497,16 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
         sL = warp_sum(sL);
         W.cnt += 1;
         W.hash += biclique_hash(*W.gp, sL, (uint64_t)kn, sR, nR);
+        emit_biclique(
+            W, kn, 32 * K,
+            [&](int b) {
+              uint32_t m = 0;
+#pragma unroll
+              for (int w = 0; w < K; ++w)
+                if (w == (b >> 5)) m = Ln[w];
+              return ((m >> (b & 31)) & 1u) != 0u;
+            },
+            [&](int b) { return src.lid[b]; });
       } else {
         W.nonmax += 1;
       }
@@ -574,6 +620,7 @@ __device__ void tier2(Warp& W, int n, int nsub, int nq, int nend, uint64_t sR0, 
   src.rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
   src.subkey = W.A64(W.sl.sub_v);
   src.lkey = W.A64(W.sl.lkey);
+  src.lid = W.A(W.sl.lid);
   full_mask(src.L0, n);
   src.nsub = nsub;
   src.nq = nq;
@@ -613,7 +660,12 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   const int nw = nsub * RS;
   for (int i = lane; i < nw; i += 32) rec[i] = __ldcg(srec + i);
   for (int i = lane; i < nsub; i += 32) subkey[i] = __ldcg(skey + i);
-  for (int i = lane; i < 32 * K; i += 32) lkey[i] = __ldcg(slk + i);
+  int32_t* lid = W.A(W.sl.lid);
+  const unsigned* sli = reinterpret_cast<const unsigned*>(sp + kSlotLid);
+  for (int i = lane; i < 32 * K; i += 32) {
+    lkey[i] = __ldcg(slk + i);
+    lid[i] = (int32_t)__ldcg(sli + i);
+  }
   __syncwarp();
   if (lane == 0) slot_free(W, slot);
   __syncwarp();
@@ -622,6 +674,7 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   src.rec = rec;
   src.subkey = subkey;
   src.lkey = lkey;
+  src.lid = lid;
   src.nsub = nsub;
   src.nq = nq;
   src.nend = nsub;
@@ -735,6 +788,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
       int j = n + __popc(bal & lanemask_lt());
       lp[j] = l;
       lkey[j] = W.gp->ukey[t.L[l]];
+      W.A(W.sl.lid)[j] = t.L[l];
     }
     n += __popc(bal);
   }
@@ -823,7 +877,10 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       if (sel) {
         int q = n + __popc(bal & lanemask_lt());
         lp[q] = l;
-        if (q < 32 * kKMax) lkey[q] = W.gp->ukey[t.L[l]];
+        if (q < 32 * kKMax) {
+          lkey[q] = W.gp->ukey[t.L[l]];
+          W.A(W.sl.lid)[q] = t.L[l];
+        }
       }
       n += __popc(bal);
     }
@@ -888,6 +945,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   if (ism) {
     W.cnt += 1;
     W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
+    emit_biclique(W, n, n, [](int) { return true; }, [&](int i) { return t.L[lp[i]]; });
   } else {
     W.nonmax += 1;
   }
@@ -908,7 +966,12 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
       subkey = slot_subkey(sp, K, ncand);
       uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
-      for (int b = lane; b < n; b += 32) lk[b] = lkey[b];
+      int32_t* li = sp + kSlotLid;
+      const int32_t* lid = W.A(W.sl.lid);
+      for (int b = lane; b < n; b += 32) {
+        lk[b] = lkey[b];
+        li[b] = lid[b];
+      }
     }
     // child indices: Q from the front, P from the back
     int nq = 0, np = 0;
@@ -1054,6 +1117,8 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       if (ism) {
         W.cnt += 1;
         W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
+        emit_biclique(W, kept, t.nL, [&](int l) { return llevel[l] == level; },
+                      [&](int l) { return t.L[l]; });
       } else {
         W.nonmax += 1;
       }
@@ -1524,6 +1589,7 @@ __device__ void run_task(Warp& W, const Task& t) {
     sL = warp_sum(sL);
     W.cnt += 1;
     W.hash += biclique_hash(g, sL, (uint64_t)nL, sR, nR);
+    emit_biclique(W, nL, nL, [](int) { return true; }, [&](int l) { return L[l]; });
   }
   bool done = nL <= 1 || np == 0;
   // ---- split (src/IterFinderGpu.cu:835-858) ----
@@ -1550,7 +1616,11 @@ __device__ void run_task(Warp& W, const Task& t) {
       // ---- tier 2 directly: masks of every candidate over all of L ----
       uint64_t* lkey = W.A64(W.sl.lkey);
       uint64_t* subkey = W.A64(W.sl.sub_v);
-      for (int l = lane; l < nL; l += 32) lkey[l] = g.ukey[L[l]];
+      int32_t* lid = W.A(W.sl.lid);
+      for (int l = lane; l < nL; l += 32) {
+        lkey[l] = g.ukey[L[l]];
+        lid[l] = L[l];
+      }
       for (int i = lane; i < nC; i += 32) subkey[i] = g.vkey[cv[i]];
       const int K = words_k(nL), RS = K + 1;
       uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));

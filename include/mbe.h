@@ -172,6 +172,16 @@ int mbe_graph_free(mbe_graph* g);
  * `params` may be NULL (defaults).  Synchronous on the calling thread. */
 int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out);
 
+/* As mbe_enumerate, also writing every maximal biclique into buf (no
+ * counterpart in the reference, which only counts): records
+ * [|U|, |V|, U ids ascending, V ids ascending] in original ids and sides,
+ * packed one after another, *used_words in all.  The kernel emits each
+ * biclique's L side into a device buffer as it is found; the host derives the
+ * other side as the common neighbourhood of L.  MBE_ERR_CAPACITY (with the
+ * records that fit, *used_words of them) when buf is too small. */
+int mbe_enumerate_emit(mbe_graph* g, const mbe_params* params, mbe_result* out, int32_t* buf,
+                       int64_t buf_words, int64_t* used_words);
+
 /* Thread-local message of the last failed call ("" if none). */
 const char* mbe_last_error_string(void);
 
