@@ -125,33 +125,69 @@ __device__ __forceinline__ void counts_done(const Warp& W, const int32_t* idx, i
 }
 
 // Emission (opt-in): appends a maximal biclique's L to the launch's record
-// buffer as [|L|, graph, internal U ids of L...]; R is N(L).  The L members
-// are the positions l < nscan with sel(l), `count` of them, id(l) each.  A
-// record that does not fit entirely is dropped (the reserved word count keeps
-// growing past the buffer, which tells the host).  The host zeroes the buffer
-// first, so a zero length word marks the end of what was written.
-template <typename Sel, typename Id>
-__device__ void emit_biclique(const Warp& W, int count, int nscan, Sel sel, Id id) {
-  int32_t* buf = W.p.emit;
-  if (!buf) return;
-  const int lane = (int)lane_id();
+// buffer as [|L|, graph, internal U ids of L...]; R is N(L).  A record that
+// does not fit entirely is dropped (the reserved word count keeps growing past
+// the buffer, which tells the host).  The host zeroes the buffer first, so a
+// zero length word marks the end of what was written.  Kept out of line and
+// given plain arguments: inlined at its four call sites, the code grew the
+// enumeration's hot loops enough to slow every launch by a quarter.
+// Reserves a record of `count` ids; -1 if it does not fit.
+__device__ __forceinline__ long long emit_reserve(EnumCtl* ctl, long long cap, int count) {
   unsigned long long pos = 0;
-  if (lane == 0) pos = atomicAdd(&W.ctl->emit_pos, (unsigned long long)count + 2);
+  if (lane_id() == 0) pos = atomicAdd(&ctl->emit_pos, (unsigned long long)count + 2);
   pos = __shfl_sync(kFull, pos, 0);
-  if (pos + (unsigned long long)count + 2 > (unsigned long long)W.p.emit_cap) return;
-  int out = 0;
-  for (int b0 = 0; b0 < nscan; b0 += 32) {
-    const int l = b0 + lane;
-    const bool s = l < nscan && sel(l);
-    const unsigned bal = __ballot_sync(kFull, s);
-    if (s) buf[pos + 2 + out + __popc(bal & lanemask_lt())] = id(l);
-    out += __popc(bal);
-  }
-  if (lane == 0) {
-    buf[pos + 1] = W.gid;
+  return pos + (unsigned long long)count + 2 > (unsigned long long)cap ? -1LL : (long long)pos;
+}
+
+__device__ __forceinline__ void emit_header(int32_t* buf, long long pos, int count, int gid) {
+  if (lane_id() == 0) {
+    buf[pos + 1] = gid;
     buf[pos] = count;
   }
   __syncwarp();
+}
+
+// L = ids[idx[i]] (or ids[i] when idx is null) for i < n.
+__device__ __noinline__ void emit_list(EnumCtl* ctl, int32_t* buf, long long cap, int gid, int n,
+                                       const int32_t* ids, const int32_t* idx) {
+  const long long pos = emit_reserve(ctl, cap, n);
+  if (pos < 0) return;
+  for (int i = (int)lane_id(); i < n; i += 32) buf[pos + 2 + i] = idx ? ids[idx[i]] : ids[i];
+  emit_header(buf, pos, n, gid);
+}
+
+// L = ids[l] for the l < nscan with llevel[l] == level, count of them.
+__device__ __noinline__ void emit_level(EnumCtl* ctl, int32_t* buf, long long cap, int gid,
+                                        int count, int nscan, const int32_t* llevel, int level,
+                                        const int32_t* ids) {
+  const long long pos = emit_reserve(ctl, cap, count);
+  if (pos < 0) return;
+  int out = 0;
+  for (int b0 = 0; b0 < nscan; b0 += 32) {
+    const int l = b0 + (int)lane_id();
+    const bool s = l < nscan && llevel[l] == level;
+    const unsigned bal = __ballot_sync(kFull, s);
+    if (s) buf[pos + 2 + out + __popc(bal & lanemask_lt())] = ids[l];
+    out += __popc(bal);
+  }
+  emit_header(buf, pos, count, gid);
+}
+
+// L = lid[b] for the set bits b of the K-word mask (m0..m3), count of them.
+__device__ __noinline__ void emit_mask(EnumCtl* ctl, int32_t* buf, long long cap, int gid,
+                                       int count, int K, uint32_t m0, uint32_t m1, uint32_t m2,
+                                       uint32_t m3, const int32_t* lid) {
+  const long long pos = emit_reserve(ctl, cap, count);
+  if (pos < 0) return;
+  const int lane = (int)lane_id();
+  int out = 0;
+  for (int w = 0; w < K; ++w) {
+    const uint32_t m = w == 0 ? m0 : (w == 1 ? m1 : (w == 2 ? m2 : m3));
+    const bool s = (m >> lane) & 1u;
+    if (s) buf[pos + 2 + out + __popc(m & lanemask_lt())] = lid[w * 32 + lane];
+    out += __popc(m);
+  }
+  emit_header(buf, pos, count, gid);
 }
 
 // Serving block of graph `gid` (a block index into the arena, which the
@@ -329,10 +365,10 @@ __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, 
     for (int w = 0; w < K; ++w) rec[(size_t)q * RS + 1 + w] = c[1 + w];
     key[q] = src.subkey[c[0] >> 8];
   }
-  int32_t* li = sp + kSlotLid;
-  for (int b = lane; b < 32 * K; b += 32) {
-    lk[b] = src.lkey[b];
-    li[b] = src.lid[b];
+  for (int b = lane; b < 32 * K; b += 32) lk[b] = src.lkey[b];
+  if (W.p.emit) {  // L ids are needed for emission only
+    int32_t* li = sp + kSlotLid;
+    for (int b = lane; b < 32 * K; b += 32) li[b] = src.lid[b];
   }
   if (lane == 0) slot_header(sp, K, nchild, nbefore, Ln, sR, nR, W.gid);
   if (slot_publish(W, slot)) return true;
@@ -368,6 +404,7 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
   uint32_t* lmask = reinterpret_cast<uint32_t*>(W.A(W.sl.lmask));
   uint64_t* rsum = W.A64(W.sl.r_sum);
   uint32_t* rcnt = reinterpret_cast<uint32_t*>(W.A(W.sl.r_cnt));
+  const bool emitting = W.p.emit != nullptr;
   const bool prune = W.p.prune != 0;
 
   for (int q = lane; q < src.nsub; q += 32) {
@@ -497,16 +534,9 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
         sL = warp_sum(sL);
         W.cnt += 1;
         W.hash += biclique_hash(*W.gp, sL, (uint64_t)kn, sR, nR);
-        emit_biclique(
-            W, kn, 32 * K,
-            [&](int b) {
-              uint32_t m = 0;
-#pragma unroll
-              for (int w = 0; w < K; ++w)
-                if (w == (b >> 5)) m = Ln[w];
-              return ((m >> (b & 31)) & 1u) != 0u;
-            },
-            [&](int b) { return src.lid[b]; });
+        if (emitting)
+          emit_mask(W.ctl, W.p.emit, W.p.emit_cap, W.gid, kn, K, Ln[0], K > 1 ? Ln[1 % K] : 0u,
+                    K > 2 ? Ln[2 % K] : 0u, K > 3 ? Ln[3 % K] : 0u, src.lid);
       } else {
         W.nonmax += 1;
       }
@@ -662,10 +692,9 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   for (int i = lane; i < nsub; i += 32) subkey[i] = __ldcg(skey + i);
   int32_t* lid = W.A(W.sl.lid);
   const unsigned* sli = reinterpret_cast<const unsigned*>(sp + kSlotLid);
-  for (int i = lane; i < 32 * K; i += 32) {
-    lkey[i] = __ldcg(slk + i);
-    lid[i] = (int32_t)__ldcg(sli + i);
-  }
+  for (int i = lane; i < 32 * K; i += 32) lkey[i] = __ldcg(slk + i);
+  if (W.p.emit)
+    for (int i = lane; i < 32 * K; i += 32) lid[i] = (int32_t)__ldcg(sli + i);
   __syncwarp();
   if (lane == 0) slot_free(W, slot);
   __syncwarp();
@@ -788,7 +817,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
       int j = n + __popc(bal & lanemask_lt());
       lp[j] = l;
       lkey[j] = W.gp->ukey[t.L[l]];
-      W.A(W.sl.lid)[j] = t.L[l];
+      if (W.p.emit) W.A(W.sl.lid)[j] = t.L[l];
     }
     n += __popc(bal);
   }
@@ -879,7 +908,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
         lp[q] = l;
         if (q < 32 * kKMax) {
           lkey[q] = W.gp->ukey[t.L[l]];
-          W.A(W.sl.lid)[q] = t.L[l];
+          if (W.p.emit) W.A(W.sl.lid)[q] = t.L[l];
         }
       }
       n += __popc(bal);
@@ -945,7 +974,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   if (ism) {
     W.cnt += 1;
     W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
-    emit_biclique(W, n, n, [](int) { return true; }, [&](int i) { return t.L[lp[i]]; });
+    if (W.p.emit) emit_list(W.ctl, W.p.emit, W.p.emit_cap, W.gid, n, t.L, lp);
   } else {
     W.nonmax += 1;
   }
@@ -966,11 +995,11 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
       rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
       subkey = slot_subkey(sp, K, ncand);
       uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
-      int32_t* li = sp + kSlotLid;
-      const int32_t* lid = W.A(W.sl.lid);
-      for (int b = lane; b < n; b += 32) {
-        lk[b] = lkey[b];
-        li[b] = lid[b];
+      for (int b = lane; b < n; b += 32) lk[b] = lkey[b];
+      if (W.p.emit) {
+        int32_t* li = sp + kSlotLid;
+        const int32_t* lid = W.A(W.sl.lid);
+        for (int b = lane; b < n; b += 32) li[b] = lid[b];
       }
     }
     // child indices: Q from the front, P from the back
@@ -1036,6 +1065,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
   const int32_t* coff = W.A(W.sl.coff);
   const int32_t* cadj = W.A(W.sl.cadj);
   const int32_t* aadj = W.A(W.sl.aadj);
+  const bool emitting = W.p.emit != nullptr;
   const int t2max = W.gp->tier2_max_l;
 
   if (lane == 0) {
@@ -1117,8 +1147,8 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       if (ism) {
         W.cnt += 1;
         W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
-        emit_biclique(W, kept, t.nL, [&](int l) { return llevel[l] == level; },
-                      [&](int l) { return t.L[l]; });
+        if (emitting)
+          emit_level(W.ctl, W.p.emit, W.p.emit_cap, W.gid, kept, t.nL, llevel, level, t.L);
       } else {
         W.nonmax += 1;
       }
@@ -1589,7 +1619,7 @@ __device__ void run_task(Warp& W, const Task& t) {
     sL = warp_sum(sL);
     W.cnt += 1;
     W.hash += biclique_hash(g, sL, (uint64_t)nL, sR, nR);
-    emit_biclique(W, nL, nL, [](int) { return true; }, [&](int l) { return L[l]; });
+    if (W.p.emit) emit_list(W.ctl, W.p.emit, W.p.emit_cap, W.gid, nL, L, nullptr);
   }
   bool done = nL <= 1 || np == 0;
   // ---- split (src/IterFinderGpu.cu:835-858) ----
@@ -1617,10 +1647,9 @@ __device__ void run_task(Warp& W, const Task& t) {
       uint64_t* lkey = W.A64(W.sl.lkey);
       uint64_t* subkey = W.A64(W.sl.sub_v);
       int32_t* lid = W.A(W.sl.lid);
-      for (int l = lane; l < nL; l += 32) {
-        lkey[l] = g.ukey[L[l]];
-        lid[l] = L[l];
-      }
+      for (int l = lane; l < nL; l += 32) lkey[l] = g.ukey[L[l]];
+      if (W.p.emit)
+        for (int l = lane; l < nL; l += 32) lid[l] = L[l];
       for (int i = lane; i < nC; i += 32) subkey[i] = g.vkey[cv[i]];
       const int K = words_k(nL), RS = K + 1;
       uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
