@@ -333,7 +333,8 @@ def main():
     consts = load_consts()
     g = gm.config_graph(WORKLOAD)
     G = gm.Graph.from_csr(g.row_off, g.col, g.nU, device=local, **FLAGS)
-    shard = dict(shard_count=world, shard_index=rank) if world > 1 else {}
+    from gmbe_b200.dist import shard_params, sum_results
+    shard = shard_params(rank, world)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     def barrier():
@@ -341,12 +342,7 @@ def main():
             dist.barrier()
 
     def reduce_result(r):
-        t = torch.tensor([int(np.int64(np.uint64(r.count))), int(np.uint64(r.set_hash).view(np.int64))],
-                         dtype=torch.int64, device=dev)
-        if world > 1:
-            dist.all_reduce(t)
-        c, h = t.tolist()
-        return int(np.int64(c).view(np.uint64)), int(np.int64(h).view(np.uint64))
+        return sum_results(r.count, r.set_hash, device=dev)
 
     def check(c, h):
         if (c, h) != (consts["count"], int(consts["set_hash"], 16)):

@@ -274,3 +274,42 @@ def test_graph_writer_matches_reference_converter(gm, tmp_path):
         theirs = tmp_path / "theirs.graph"
         subprocess.run([conv, str(adj), str(theirs)], check=True, capture_output=True)
         assert ours.read_bytes() == theirs.read_bytes()
+
+
+def _shard_rank(rank, world, port, graph, out):
+    # One rank of the N>1 path, the CPU oracle standing in for its GPU: its
+    # share of the roots (the strided positions mbe_params shard_* selects),
+    # then the same reduction bench.py uses.
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from gmbe_b200.dist import shard_params, sum_results
+        ro, co, nU = graph
+        p = shard_params(rank, world)
+        r = oracle.gmbe_strided(ro, co, nU, p["shard_index"], p["shard_count"], threads=1)
+        out[rank] = sum_results(r.count, r.set_hash)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_ranks_sum_to_the_whole_graph():
+    import socket
+    import torch.multiprocessing as mp
+    graph = planted(300, 200, blocks=6, seed=3, bsize=14)
+    want = oracle.gmbe(*graph)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_shard_rank, args=(r, 2, port, graph, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    assert out[0] == out[1] == (want.count, want.set_hash)
+    # each share alone is a strict part of the whole
+    half = oracle.gmbe_strided(*graph, 0, 2)
+    assert 0 < half.count < want.count

@@ -200,3 +200,22 @@ def test_root_parts_do_not_change_result(gm, work, chunk):
             assert (r.count, r.set_hash) == (want.count, want.set_hash)
             if work == 1 and chunk == 2:
                 assert r.tasks_split > 0
+
+
+@pytest.mark.parametrize("world", [2, 3, 8])
+def test_shards_match_oracle_and_add_up(gm, world):
+    # The N>1 path: rank r enumerates the roots at positions p = r mod world
+    # from the top of the internal order; each share matches the oracle's and
+    # the shares sum (mod 2^64) to the whole graph.
+    from gmbe_b200.dist import shard_params
+    g = gm.config_graph("small")
+    with gm.Graph.from_csr(g.row_off, g.col, g.nU, uvtrans=1) as G:
+        full = G.enumerate()
+        tot_c, tot_h = 0, 0
+        for rank in range(world):
+            r = G.enumerate(**shard_params(rank, world))
+            o = oracle.gmbe_strided(g.row_off, g.col, g.nU, rank, world, uvtrans=1)
+            assert (r.count, r.set_hash) == (o.count, o.set_hash)
+            tot_c += r.count
+            tot_h = (tot_h + r.set_hash) % (1 << 64)
+    assert (full.count, full.set_hash) == (tot_c, tot_h)
