@@ -117,6 +117,8 @@ _sig = {
     "mbe_graph_from_adj": (C.c_int, [C.c_char_p, C.POINTER(Opts), C.POINTER(C.c_void_p)]),
     "mbe_graph_from_csr": (C.c_int, [_P32, _P32, C.c_int32, C.c_int32, C.c_int64,
                                      C.POINTER(Opts), C.POINTER(C.c_void_p)]),
+    "mbe_graph_build_on_device": (C.c_int, [_P32, _P32, C.c_int32, C.c_int32, C.c_int64,
+                                            C.POINTER(Opts), C.POINTER(C.c_void_p)]),
     "mbe_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(GraphInfo)]),
     "mbe_graph_free": (C.c_int, [C.c_void_p]),
     "mbe_enumerate": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]),
@@ -205,6 +207,19 @@ class Graph:
         opts = make_opts(uvtrans, order, fast_mode, device)
         _check(_lib.mbe_graph_from_csr(_ptr(ro), _ptr(co), len(ro) - 1, int(nU), len(co),
                                        C.byref(opts), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def build_on_device(cls, row_off, col, nU: int = 0, uvtrans=0, order=1, fast_mode=1,
+                        device=0):
+        """from_csr with the transposes, ordering, keys and capacities computed
+        on the GPU (mbe_graph_build_on_device); rows of equal degree keep their
+        input order, which leaves the enumerated set unchanged."""
+        ro, co = _i32(row_off), _i32(col)
+        h = C.c_void_p()
+        opts = make_opts(uvtrans, order, fast_mode, device)
+        _check(_lib.mbe_graph_build_on_device(_ptr(ro), _ptr(co), len(ro) - 1, int(nU), len(co),
+                                              C.byref(opts), C.byref(h)))
         return cls(h.value)
 
     @classmethod

@@ -13,19 +13,6 @@
 
 using namespace gmbe;
 
-struct mbe_graph {
-  HostGraph h;
-  mbe_opts opts;
-  int device = 0;
-  int32_t* d_row_off = nullptr;
-  int32_t* d_col = nullptr;
-  int32_t* d_rev_off = nullptr;
-  int32_t* d_rev_col = nullptr;
-  uint64_t* d_ukey = nullptr;
-  uint64_t* d_vkey = nullptr;
-  // Capacities derived from the graph (max over roots).
-  int32_t capS = 0, capL = 0;
-};
 
 namespace {
 
@@ -403,6 +390,31 @@ int mbe_graph_from_csr(const int32_t* row_off, const int32_t* col, int32_t nV, i
   return finish_graph(g, out);
 }
 
+int mbe_graph_build_on_device(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t nU,
+                              int64_t nE, const mbe_opts* opts, mbe_graph** out) {
+  clear_error();
+  if (!out) return set_error(MBE_ERR_INVALID, "null output handle");
+  *out = nullptr;
+  mbe_opts o;
+  if (opts) o = *opts;
+  else mbe_opts_default(&o);
+  // The two-hop statistics (and the -o 3 peeling order they come with) are
+  // host work: without fast_mode the graph is built as mbe_graph_from_csr does.
+  if (!o.fast_mode) return mbe_graph_from_csr(row_off, col, nV, nU, nE, &o, out);
+  if (o.device < 0 || o.device >= kMaxDevices) return set_error(MBE_ERR_INVALID, "bad device");
+  mbe_graph* g = new mbe_graph();
+  g->opts = o;
+  g->device = o.device;
+  int rc = device_build_graph(g, row_off, col, nV, nU, nE);
+  if (rc) {
+    free_device(g);
+    delete g;
+    return rc;
+  }
+  *out = g;
+  return MBE_OK;
+}
+
 int mbe_graph_from_adj(const char* path, const mbe_opts* opts, mbe_graph** out) {
   clear_error();
   if (!path || !out) return set_error(MBE_ERR_INVALID, "null argument");
@@ -557,6 +569,7 @@ int mbe_enumerate_emit(mbe_graph* g, const mbe_params* params, mbe_result* out, 
   if (rc) return rc;
   // Records: R = N(L) from the internal U -> V lists; both sides to original
   // ids (internal U is the original V side when -t swapped them).
+  if ((rc = ensure_host_csr(g))) return rc;
   const HostGraph& h = g->h;
   std::vector<int32_t> L, R, tmp, us, vs;
   size_t pos = 0;

@@ -42,6 +42,35 @@ struct Workspace {
 
 Workspace& workspace(int device);
 
+}  // namespace gmbe
+
+// A graph handle (include/mbe.h): the internal graph on the host and device.
+struct mbe_graph {
+  gmbe::HostGraph h;  // built on the device: sizes, degrees and v_orig/u_orig only
+  mbe_opts opts;
+  int device = 0;
+  bool device_built = false;  // host CSR arrays are fetched when needed (emission)
+  int32_t* d_row_off = nullptr;
+  int32_t* d_col = nullptr;
+  int32_t* d_rev_off = nullptr;
+  int32_t* d_rev_col = nullptr;
+  uint64_t* d_ukey = nullptr;
+  uint64_t* d_vkey = nullptr;
+  // Capacities derived from the graph (max over roots).
+  int32_t capS = 0, capL = 0;
+};
+
+namespace gmbe {
+
+// Builds g's internal graph on its device from an .adj-shaped host CSR (the
+// -t swap, -o 0/1/2 ordering, both CSRs, hash keys, capacities); fills the
+// host fields sizes, degrees, swapped, v_orig, u_orig.
+int device_build_graph(mbe_graph* g, const int32_t* row_off, const int32_t* col, int32_t nV,
+                       int32_t nU, int64_t nE);
+
+// Fetches the host CSR copies of a graph built on the device (no-op otherwise).
+int ensure_host_csr(mbe_graph* g);
+
 // What one launch needs from the workspace: the largest internal V side (the
 // count maps) and the per-warp capacities, maxima over the launch's graphs.
 struct LaunchSpec {

@@ -161,6 +161,18 @@ int mbe_graph_from_adj(const char* path, const mbe_opts* opts, mbe_graph** out);
 int mbe_graph_from_csr(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t nU,
                        int64_t nE, const mbe_opts* opts, mbe_graph** out);
 
+/* Same input, checks and result as mbe_graph_from_csr, with the build on the
+ * device: the input CSR is uploaded once and the transposes, the -t swap, the
+ * -o 1/2 degree ordering, the hash keys and the capacities are computed there
+ * (no reference counterpart; the reference builds on the host in
+ * CSRBiGraph::Read, src/BiGraph.cu:13-278).  Rows of equal degree keep their
+ * input order instead of the reference's lexicographic tie-break; the set of
+ * maximal bicliques (count and set hash) is the same.  Without fast_mode the
+ * two-hop statistics are host work, and the call builds as
+ * mbe_graph_from_csr does.  nV = 0 or nE = 0 is MBE_ERR_INVALID here. */
+int mbe_graph_build_on_device(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t nU,
+                              int64_t nE, const mbe_opts* opts, mbe_graph** out);
+
 int mbe_graph_get_info(const mbe_graph* g, mbe_graph_info* info);
 
 /* Release host and device memory.  Replaces CSRBiGraph::Reset (src/BiGraph.cu:433-454). */
