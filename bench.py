@@ -189,6 +189,22 @@ def run_profile_case():
                       "set_hash": f"{b.set_hash:#x}", "kernel_ms": b.kernel_ms}), flush=True)
 
 
+def run_profile_full():
+    """The bench's own launch for one-pass ncu metrics (DRAM bytes): the whole
+    medium graph with the default parameters, one warm-up and one profiled
+    enumeration, both checked against the known count and set hash."""
+    import gmbe_b200 as gm
+    consts = load_consts()
+    g = gm.config_graph(WORKLOAD)
+    with gm.Graph.from_csr(g.row_off, g.col, g.nU, **FLAGS) as G:
+        rs = [G.enumerate() for _ in range(2)]
+    for r in rs:
+        if (r.count, f"{r.set_hash:#x}") != (consts["count"], consts["set_hash"]):
+            raise SystemExit(f"full launch mismatch: {r.count} {r.set_hash:#x}")
+    print(json.dumps({"profile_case": "medium, full launch", "count": rs[1].count,
+                      "set_hash": f"{rs[1].set_hash:#x}", "kernel_ms": rs[1].kernel_ms}), flush=True)
+
+
 def batched_leg(n=4096, replays=3, plain_stride=4):
     """Batched workload: n graphs of the batched distribution (seeds 1000..)
     in one persistent launch replayed from a CUDA graph, against one plain
@@ -292,6 +308,29 @@ def serving_leg(n=1000, rates=(1000, 5000, 20000)):
             "results_equal_plain": all(o == plain for o in outs)}
 
 
+SERVING_LIMIT_S = 420
+
+
+def serving_leg_isolated(limit_s=SERVING_LIMIT_S):
+    """serving_leg in a child process (its own CUDA context) under a hard time
+    limit: a server that stalls cannot keep this run from printing its line.
+    The child's progress goes to stderr as usual; its result is the last line
+    of its stdout."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--serving-leg"]
+    try:
+        p = subprocess.run(cmd, stdout=subprocess.PIPE, text=True, timeout=limit_s)
+    except subprocess.TimeoutExpired:
+        log(f"serving: no result within {limit_s} s; child stopped")
+        return {"error": f"serving leg did not finish within {limit_s} s"}
+    lines = [x for x in (p.stdout or "").splitlines() if x.strip()]
+    if p.returncode != 0 or not lines:
+        return {"error": f"serving leg exited with status {p.returncode}"}
+    try:
+        return json.loads(lines[-1])
+    except ValueError:
+        return {"error": "serving leg printed no result"}
+
+
 def WORKLOAD_DESC():
     import gmbe_b200 as gm
     return gm.DESCRIPTIONS[WORKLOAD]
@@ -308,12 +347,22 @@ def main():
                     help="skip the batched and serving legs (they run at N=1 only)")
     ap.add_argument("--profile", action="store_true",
                     help="one reduced launch for ncu: 16 blocks, every 64th root (~1.6 GB scratch)")
+    ap.add_argument("--profile-full", action="store_true",
+                    help="the full medium launch for one-pass ncu metrics (DRAM bytes)")
+    ap.add_argument("--serving-leg", action="store_true",
+                    help="run only the serving leg and print its result (used by the N=1 run)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
         return
     if args.profile:
         run_profile_case()
+        return
+    if args.profile_full:
+        run_profile_full()
+        return
+    if args.serving_leg:
+        print(json.dumps(serving_leg()), flush=True)
         return
 
     import numpy as np
@@ -441,7 +490,7 @@ def main():
         }
         if world == 1 and not args.no_extras:
             line["batched"] = batched_leg()
-            line["serving"] = serving_leg()
+            line["serving"] = serving_leg_isolated()
         if world == 1 and not args.no_cpu_baseline:
             log("CPU baseline")
             v, sample, cores = cpu_sample(g)

@@ -28,7 +28,11 @@ inline size_t enum_smem_bytes(const ScratchLayout& sl) {
   return (size_t)sl.seen_words * sizeof(uint32_t) * kEnumWarps;
 }
 // |P|*|L| from which a child is shared out while many warps wait for work.
-constexpr int32_t kShareMinWorkDefault = 64;
+constexpr int32_t kShareMinWorkDefault = 256;
+// The same floor for a serving launch.  It stays at 64: the serving path was
+// exercised under load at 64, and the one loaded serving run at 256 stalled
+// without a found cause.
+constexpr int32_t kServeShareMinWorkDefault = 64;
 // P candidates per part of a root split into parts.
 constexpr int32_t kRangeChunkDefault = 64;
 
