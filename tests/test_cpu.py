@@ -213,6 +213,34 @@ def test_csr_validation_runs_before_any_device_call(gm):
     assert ei.value.name == "MBE_ERR_FORMAT"
 
 
+@pytest.mark.parametrize("ro,code", [
+    ([0, 2, 2, 3], "MBE_ERR_FORMAT"),   # empty row
+    ([1, 2, 3, 3], "MBE_ERR_FORMAT"),   # row_off[0] != 0
+    ([0, 2, 3, 4], "MBE_ERR_FORMAT"),   # row_off[nV] != nE
+    ([0, 3, 2, 3], "MBE_ERR_FORMAT"),   # decreasing offsets
+    ([0], "MBE_ERR_INVALID"),           # no rows
+])
+def test_device_build_checks_offsets_before_any_device_call(gm, ro, code):
+    # mbe_graph_build_on_device reads through the row offsets only after the
+    # host has checked them; malformed offsets never reach a kernel.
+    co = np.array([0, 1, 2], np.int32)
+    with pytest.raises(gm.MBEError) as ei:
+        gm.Graph.build_on_device(np.array(ro, np.int32), co, 3)
+    assert ei.value.name == code
+
+
+def test_bench_serving_leg_reports_instead_of_hanging():
+    # The serving leg runs in a child process under a hard limit: a child that
+    # outlives the limit, or fails, becomes an error entry of the bench line.
+    import bench
+    out = bench.serving_leg_isolated(limit_s=1)
+    assert out == {"error": "serving leg did not finish within 1 s"}
+    import torch
+    if not torch.cuda.is_available():
+        out = bench.serving_leg_isolated(limit_s=300)
+        assert set(out) == {"error"} and "exited with status" in out["error"]
+
+
 def test_params_defaults(gm):
     p = gm.default_params()
     assert (p.bound_height, p.bound_size, p.prune) == (20, 1500, 1)
