@@ -436,10 +436,11 @@ def main():
     # Each call uploads the .adj-shaped CSR once and builds the graph on the
     # device (mbe_graph_build_on_device), then enumerates; it reads back the
     # build's checks (8 B), its capacities (24 B), the internal row order
-    # (4 B per internal V vertex), the launch's control block and the result.
+    # (4 B per internal V vertex), the launch's control block (208 B) and the
+    # result (24 B).
     iV = min(g.nV, g.nU) if FLAGS["uvtrans"] == 1 else g.nV
     h2d = 4 * ((g.nV + 1) + g.nE)
-    d2h = 8 + 24 + 4 * iV + 176 + 24
+    d2h = 8 + 24 + 4 * iV + 208 + 24
     G.free()
 
     def e2e_leg(build):

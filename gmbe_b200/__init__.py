@@ -60,7 +60,8 @@ class Params(C.Structure):
                 ("split_mode", C.c_int32), ("direct_max_c", C.c_int32),
                 ("root_split_size", C.c_int32), ("share_min_work", C.c_int32),
                 ("range_split_work", C.c_int32), ("range_chunk", C.c_int32),
-                ("eager_share", C.c_int32)]
+                ("eager_share", C.c_int32), ("big_two_hop", C.c_int32),
+                ("big_warps", C.c_int32)]
 
 
 class Result(C.Structure):

@@ -199,17 +199,29 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   int dev_sms = 0;
   CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, spec.device));
   int occ = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ, spec.n_big > 0 ? mbe_enum_kernel_tiers : mbe_enum_kernel, kEnumThreads, 0));
   if (occ < 1) return set_error(MBE_ERR_CUDA, "enumeration kernel cannot be resident");
   plan->blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * occ) : dev_sms * occ;
   plan->warps = plan->blocks * kEnumWarps;
   if (spec.capC >= (1 << 24))
     return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
   plan->sl = make_layout(spec.map_words, spec.capC, spec.capL, spec.capS);
-  CK(cudaFuncSetAttribute(mbe_enum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // The big tier (if any): the first n_big warps.  Both layouts share the
+  // count-map size, hence the shared-memory bitmap.
+  const int n_big = std::max(0, std::min(spec.n_big, plan->warps));
+  ScratchLayout big_sl;
+  memset(&big_sl, 0, sizeof(big_sl));
+  if (n_big > 0) {
+    if (spec.bigC >= (1 << 24))
+      return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
+    big_sl = make_layout(spec.map_words, spec.bigC, spec.bigL, spec.bigS);
+  }
+  CK(cudaFuncSetAttribute(n_big > 0 ? mbe_enum_kernel_tiers : mbe_enum_kernel,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)enum_smem_bytes(plan->sl)));
   plan->map_words = spec.map_words;
-  size_t need = (size_t)plan->sl.words_per_warp * (size_t)plan->warps * sizeof(int32_t);
+  size_t need = scratch_bytes(plan->sl, big_sl, plan->warps, n_big);
   if (need > ws.scratch_bytes) {
     cudaFree(ws.scratch);
     ws.scratch = nullptr;
@@ -224,7 +236,8 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   // Every task leaves its warp's dense count map all-zero.  A different
   // layout puts the maps elsewhere: they are cleared (strided, maps only).
   plan->clear_maps = ws.map_pitch_words != plan->sl.words_per_warp ||
-                     ws.map_words != spec.map_words || ws.map_warps < plan->warps;
+                     ws.map_words != spec.map_words || ws.map_warps < plan->warps ||
+                     ws.map_big != n_big || ws.map_big_pitch != big_sl.words_per_warp;
   int32_t qcap = prm.queue_capacity > 0
                      ? prm.queue_capacity
                      : (int32_t)std::min<int64_t>(1 << 22,
@@ -278,6 +291,12 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   apply_range_split(prm, &ep.range_work, &ep.range_chunk);
   ep.eager_share = eager_share_of(prm);
   ep.n_graphs = spec.n_graphs;
+  ep.n_big_warps = n_big;
+  ep.big_sl = big_sl;
+  if (n_big > 0) {  // vertex-tuple children and root parts could need the big tier
+    ep.root_split = 0;
+    ep.range_work = 0;
+  }
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;
   plan->pool.nslot = prm.split_mode == 1 ? 0 : ws.nslot;
@@ -286,12 +305,21 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
 
 int engine_clear_maps(Workspace& ws, LaunchPlan* plan, cudaStream_t st) {
   if (!plan->clear_maps) return MBE_OK;
-  CK(cudaMemset2DAsync(ws.scratch, (size_t)plan->sl.words_per_warp * sizeof(int32_t), 0,
-                       (size_t)std::max<int32_t>(plan->map_words, 1) * sizeof(int32_t),
-                       (size_t)plan->warps, st));
+  // The count map is the first slice of either layout.
+  const size_t width = (size_t)std::max<int32_t>(plan->map_words, 1) * sizeof(int32_t);
+  const int n_big = plan->ep.n_big_warps;
+  const size_t big_pitch = (size_t)plan->ep.big_sl.words_per_warp;
+  if (n_big > 0)
+    CK(cudaMemset2DAsync(ws.scratch, big_pitch * sizeof(int32_t), 0, width, (size_t)n_big, st));
+  if (plan->warps > n_big)
+    CK(cudaMemset2DAsync(ws.scratch + big_pitch * (size_t)n_big,
+                         (size_t)plan->sl.words_per_warp * sizeof(int32_t), 0, width,
+                         (size_t)(plan->warps - n_big), st));
   ws.map_pitch_words = plan->sl.words_per_warp;
   ws.map_words = plan->map_words;
   ws.map_warps = plan->warps;
+  ws.map_big = n_big;
+  ws.map_big_pitch = (int64_t)big_pitch;
   plan->clear_maps = false;
   return MBE_OK;
 }
@@ -306,9 +334,10 @@ int engine_enqueue(Workspace& ws, LaunchPlan* plan, const DevGraph* d_graphs,
   CK(cudaMemsetAsync(ws.slot_bits, 0, sizeof(uint32_t) * (size_t)(ws.nslot / 32), st));
   CK(cudaMemsetAsync(d_gres, 0, 3 * sizeof(unsigned long long) * (size_t)n_graphs, st));
   if (ev0) CK(cudaEventRecord(ev0, st));
-  mbe_enum_kernel<<<plan->blocks, kEnumThreads, enum_smem_bytes(plan->sl), st>>>(d_graphs, d_prefix, d_gres, plan->ep,
-                                                          plan->sl, ws.ctl, ws.q_tasks, ws.q_seq,
-                                                          plan->pool, ws.scratch, ws.exit_ns);
+  auto* kernel = plan->ep.n_big_warps > 0 ? mbe_enum_kernel_tiers : mbe_enum_kernel;
+  kernel<<<plan->blocks, kEnumThreads, enum_smem_bytes(plan->sl), st>>>(
+      d_graphs, d_prefix, d_gres, plan->ep, plan->sl, ws.ctl, ws.q_tasks, ws.q_seq, plan->pool,
+      ws.scratch, ws.exit_ns);
   CK(cudaGetLastError());
   if (ev1) CK(cudaEventRecord(ev1, st));
   return MBE_OK;
@@ -450,6 +479,111 @@ int mbe_graph_free(mbe_graph* g) {
   return MBE_OK;
 }
 
+namespace {
+
+// Whether one scratch layout for every warp fits the device, and if not (or
+// when prm.big_two_hop asks for it) the two tiers: small warps sized for
+// roots whose two-hop multiset is at most T, and spec->n_big warps sized for
+// the largest root, which take the listed roots (this launch's roots above T,
+// in claim order).  flags[v] marks a listed root.
+int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t re, int32_t si, int32_t sc,
+                   int32_t n_roots, size_t reusable_bytes, LaunchSpec* spec,
+                   std::vector<int32_t>* list, std::vector<uint8_t>* flags) {
+  const HostGraph& h0 = g->h;
+  const int32_t nV = std::max<int32_t>(h0.V_size, 1);
+  int dev_sms = 0, occ = 0;
+  CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
+  const int blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * std::max(occ, 1))
+                                    : dev_sms * std::max(occ, 1);
+  const int warps = blocks * kEnumWarps;
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  // What the scratch may take: free memory plus the scratch the workspace
+  // already holds, less room for the queue, slots and the caller's arrays.
+  const size_t reserve = ((size_t)2 << 30) + total_b / 50;
+  const size_t avail = free_b + reusable_bytes;
+  const size_t budget = avail > reserve ? avail - reserve : 0;
+  const ScratchLayout full = make_layout(nV, spec->capC, spec->capL, spec->capS);
+  const size_t full_bytes = (size_t)full.words_per_warp * sizeof(int32_t);
+  if (prm.big_two_hop <= 0 && full_bytes * (size_t)warps <= budget) return MBE_OK;
+  if (prm.split_mode == 1)
+    return set_error(MBE_ERR_INVALID, "split_mode 1 needs one scratch tier for every warp");
+
+  // Two-hop multiset and degree of every root of this launch.
+  int rc = ensure_host_csr(g);
+  if (rc) return rc;
+  const HostGraph& h = g->h;
+  std::vector<int64_t> S((size_t)n_roots);
+  std::vector<int32_t> D((size_t)n_roots);
+  for (int32_t k = 0; k < n_roots; ++k) {
+    const int32_t v = re - 1 - (si + k * sc);
+    int64_t s = 0;
+    for (int32_t i = h.row_off[v]; i < h.row_off[v + 1]; ++i) {
+      const int32_t u = h.col[i];
+      s += h.rev_off[u + 1] - h.rev_off[u];
+    }
+    S[(size_t)k] = s;
+    D[(size_t)k] = h.row_off[v + 1] - h.row_off[v];
+  }
+  // The small tier must hold any exported sub-problem a big warp makes.
+  const int32_t min_c = std::min<int32_t>(spec->capC, kSlotMaxRecords);
+  auto small_layout = [&](int64_t T) {
+    int32_t capL = 1;
+    for (int32_t k = 0; k < n_roots; ++k)
+      if (S[(size_t)k] <= T) capL = std::max(capL, D[(size_t)k]);
+    const int32_t capS = (int32_t)std::max<int64_t>(1, std::min<int64_t>(T, spec->capS));
+    const int32_t capC = std::max(min_c, std::max<int32_t>(1, std::min<int32_t>(nV, capS)));
+    return make_layout(nV, capC, std::min(capL, spec->capL), capS);
+  };
+  int64_t T = prm.big_two_hop;
+  if (T <= 0) {
+    // The largest power of two from 2^16 whose small tier leaves 40 % of the
+    // budget to the big warps.
+    T = (int64_t)1 << 16;
+    for (int64_t t = T; t < spec->capS; t <<= 1)
+      if ((size_t)small_layout(t).words_per_warp * sizeof(int32_t) * (size_t)warps <=
+          budget / 10 * 6)
+        T = t;
+  }
+  list->clear();
+  flags->assign((size_t)nV, 0);
+  for (int32_t k = 0; k < n_roots; ++k)
+    if (S[(size_t)k] > T) {
+      const int32_t v = re - 1 - (si + k * sc);
+      list->push_back(v);
+      (*flags)[(size_t)v] = 1;
+    }
+  if (list->empty()) {  // every root fits the small bound: one tier as usual
+    flags->clear();
+    return MBE_OK;
+  }
+  const ScratchLayout small = small_layout(T);
+  const size_t small_b = (size_t)small.words_per_warp * sizeof(int32_t);
+  if (small_b * (size_t)warps > budget)
+    return set_error(MBE_ERR_NOMEM, "scratch of %d warps at two-hop bound %lld: %.2f GB of %.2f GB",
+                     warps, (long long)T, small_b * (double)warps / 1e9, budget / 1e9);
+  const size_t extra = full_bytes > small_b ? full_bytes - small_b : 0;
+  const int64_t fit = extra ? (int64_t)((budget - small_b * (size_t)warps) / extra) : warps;
+  int64_t n_big = prm.big_warps > 0
+                      ? prm.big_warps
+                      : std::min<int64_t>({(int64_t)list->size(), fit, (int64_t)warps / 2});
+  n_big = std::min<int64_t>(n_big, warps);
+  if (n_big < 1 || n_big > fit)
+    return set_error(MBE_ERR_NOMEM, "%lld warps for the largest roots (%.2f GB each) do not fit",
+                     (long long)std::max<int64_t>(n_big, 1), full_bytes / 1e9);
+  spec->n_big = (int32_t)n_big;
+  spec->bigC = spec->capC;
+  spec->bigL = spec->capL;
+  spec->bigS = spec->capS;
+  spec->capC = small.capC;
+  spec->capL = small.capL;
+  spec->capS = small.capS;
+  return MBE_OK;
+}
+
+}  // namespace
+
 // mbe_enumerate, optionally writing biclique records into d_emit (emit_cap
 // words) and reporting the words reserved in *emit_pos.
 static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* out,
@@ -501,10 +635,37 @@ static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* o
   spec.capL = g->capL;
   spec.capS = g->capS;
   spec.n_graphs = 1;
+  std::vector<int32_t> big_list;
+  std::vector<uint8_t> big_flags;
+  if ((rc = plan_two_tiers(g, prm, re, si, sc, n_roots, ws.scratch_bytes, &spec, &big_list,
+                           &big_flags)))
+    return rc;
   LaunchPlan plan;
   if ((rc = engine_prepare(ws, spec, prm, &plan))) return rc;
   plan.ep.emit = d_emit;
   plan.ep.emit_cap = emit_cap;
+  if (plan.ep.n_big_warps > 0) {
+    if (big_list.size() > ws.big_roots_cap) {
+      cudaFree(ws.big_roots);
+      ws.big_roots = nullptr;
+      ws.big_roots_cap = 0;
+      CK(cudaMalloc((void**)&ws.big_roots, sizeof(int32_t) * big_list.size()));
+      ws.big_roots_cap = big_list.size();
+    }
+    if (big_flags.size() > ws.big_flag_cap) {
+      cudaFree(ws.big_flag);
+      ws.big_flag = nullptr;
+      ws.big_flag_cap = 0;
+      CK(cudaMalloc((void**)&ws.big_flag, big_flags.size()));
+      ws.big_flag_cap = big_flags.size();
+    }
+    CK(cudaMemcpyAsync(ws.big_roots, big_list.data(), sizeof(int32_t) * big_list.size(),
+                       cudaMemcpyHostToDevice, 0));
+    CK(cudaMemcpyAsync(ws.big_flag, big_flags.data(), big_flags.size(), cudaMemcpyHostToDevice, 0));
+    plan.ep.n_big_roots = (int32_t)big_list.size();
+    plan.ep.big_roots = ws.big_roots;
+    plan.ep.big_flag = ws.big_flag;
+  }
   long long prefix[2] = {0, n_roots};
   CK(cudaMemcpyAsync(ws.d_graph1, &dg, sizeof(dg), cudaMemcpyHostToDevice, 0));
   CK(cudaMemcpyAsync(ws.d_prefix1, prefix, sizeof(prefix), cudaMemcpyHostToDevice, 0));

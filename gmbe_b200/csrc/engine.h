@@ -32,9 +32,16 @@ struct Workspace {
   DevGraph* d_graph1 = nullptr;
   long long* d_prefix1 = nullptr;
   unsigned long long* d_gres1 = nullptr;
-  // Layout the per-warp count maps were last cleared for.
+  // Layout the per-warp count maps were last cleared for (big tier: the
+  // first map_big warps, pitch map_big_pitch).
   int64_t map_pitch_words = -1, map_words = -1;
   int32_t map_warps = -1;
+  int64_t map_big_pitch = 0;
+  int32_t map_big = 0;
+  // Two-tier launches: the big-root list and the per-root flags.
+  int32_t* big_roots = nullptr;
+  uint8_t* big_flag = nullptr;
+  size_t big_roots_cap = 0, big_flag_cap = 0;
   // Bumped whenever a buffer above is (re)allocated: a captured launch that
   // refers to an older generation must be captured again.
   uint64_t gen = 1;
@@ -78,16 +85,28 @@ struct LaunchSpec {
   int32_t map_words = 1;
   int32_t capC = 1, capL = 1, capS = 1;
   int32_t n_graphs = 1;
+  // Two tiers (single-graph launches): n_big warps with these capacities,
+  // the others with capC/capL/capS above.  n_big == 0: one tier.
+  int32_t n_big = 0;
+  int32_t bigC = 1, bigL = 1, bigS = 1;
 };
 
 struct LaunchPlan {
   int blocks = 0, warps = 0;
   ScratchLayout sl;
-  EnumParams ep;
+  EnumParams ep;  // ep.n_big_warps / ep.big_sl: the big tier, if any
   SlotPool pool;
   bool clear_maps = false;
   int32_t map_words = 1;
 };
+
+// Device bytes of the scratch of `warps` warps, n_big of them with the big
+// layout (n_big == 0: every warp with sl).
+inline size_t scratch_bytes(const ScratchLayout& sl, const ScratchLayout& big, int warps,
+                            int n_big) {
+  return ((size_t)big.words_per_warp * (size_t)n_big +
+          (size_t)sl.words_per_warp * (size_t)(warps - n_big)) * sizeof(int32_t);
+}
 
 // Allocates or grows the workspace and fixes the launch shape (host-only,
 // not capturable).  Caller holds ws.mu.

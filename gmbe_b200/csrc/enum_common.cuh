@@ -71,6 +71,7 @@ struct EnumCtl {
   unsigned long long max_task_shape;  // its |C| | part << 32 | parts << 48 (root tasks)
   unsigned long long n_tasks, n_tier2;
   unsigned long long emit_pos;  // words of biclique records reserved (may pass the buffer's end)
+  long long next_big;           // entries of the big-root list handed out so far
 };
 
 // Per-warp scratch layout (int32 words unless noted), offsets in words from
@@ -157,6 +158,16 @@ struct EnumParams {
   long long emit_cap;         // words in emit
   int32_t server;             // 1: graphs arrive while the launch runs (ServeLink)
   ServeLink serve;
+  // Two scratch tiers (single-graph launches only).  Warps [0, n_big_warps)
+  // use big_sl and first take the roots of big_roots (internal ids, in claim
+  // order); every other warp uses the launch's layout.  Roots flagged in
+  // big_flag (indexed by internal V id) are in that list and are skipped when
+  // met through the ordinary root counter.  n_big_warps == 0: one tier.
+  int32_t n_big_warps;
+  int32_t n_big_roots;
+  const int32_t* big_roots;
+  const uint8_t* big_flag;
+  ScratchLayout big_sl;
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

@@ -250,6 +250,9 @@ constexpr int kSlotRec = kSlotLid + 32 * 4;
 __host__ __device__ constexpr int slot_cap(int K) {
   return ((kSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
 }
+static_assert(slot_cap(1) == kSlotMaxRecords && slot_cap(1) >= slot_cap(2) &&
+                  slot_cap(2) >= slot_cap(4) && kSlotWords == kSlotWordsHost,
+              "host view of the slot size");
 // header words: 0 K, 1 nsub, 2 nq, 3 graph, 4..7 L0, 8..9 sR0, 10 nR0
 __device__ __forceinline__ uint64_t* slot_subkey(int32_t* sp, int K, int nsub) {
   return reinterpret_cast<uint64_t*>(sp + kSlotRec + ((nsub * (K + 1) + 1) & ~1));
@@ -1819,23 +1822,33 @@ __device__ void serve_task_done(Warp& W, int32_t gid) {
   d->seq = pos + 1;
 }
 
-__global__ void __launch_bounds__(kEnumThreads, 1)
-    mbe_enum_kernel(const DevGraph* graphs, const long long* root_prefix,
-                    unsigned long long* gres, const __grid_constant__ EnumParams p,
-                    const __grid_constant__ ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
-                    unsigned long long* q_seq, SlotPool pool, int32_t* scratch,
-                    unsigned long long* exit_ns) {
+// The persistent loop.  kTiers: the launch has a big tier (p.n_big_warps >
+// 0); without it every warp uses `sl` and the tier code compiles away.
+template <bool kTiers>
+__device__ __forceinline__ void enum_main(const DevGraph* graphs, const long long* root_prefix,
+                                          unsigned long long* gres, const EnumParams& p,
+                                          const ScratchLayout& sl, EnumCtl* ctl, Task* q_tasks,
+                                          unsigned long long* q_seq, const SlotPool& pool,
+                                          int32_t* scratch, unsigned long long* exit_ns) {
   uint64_t t_start = globaltimer_ns();
   const int lane = (int)lane_id();
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  Warp W{p, sl};
+  // Two tiers: the first n_big_warps warps hold the big layout, then the
+  // launch's layout follows for every other warp.
+  const bool big = kTiers && warp_global < p.n_big_warps;
+  Warp W{p, (kTiers && big) ? p.big_sl : sl};
   W.ctl = ctl;
   W.q_tasks = q_tasks;
   W.q_seq = q_seq;
   W.slots = pool.slots;
   W.slot_bits = pool.bits;
   W.nslot = pool.nslot;
-  W.base = scratch + (size_t)warp_global * (size_t)sl.words_per_warp;
+  if (!kTiers)
+    W.base = scratch + (size_t)warp_global * (size_t)sl.words_per_warp;
+  else
+    W.base = big ? scratch + (size_t)warp_global * (size_t)p.big_sl.words_per_warp
+                 : scratch + (size_t)p.n_big_warps * (size_t)p.big_sl.words_per_warp +
+                       (size_t)(warp_global - p.n_big_warps) * (size_t)sl.words_per_warp;
   extern __shared__ uint32_t enum_smem[];
   W.seen = sl.seen_words ? enum_smem + (size_t)(threadIdx.x >> 5) * sl.seen_words : nullptr;
   if (W.seen) {
@@ -1867,20 +1880,43 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
       have = queue_pop(W, &t) ? 1 : 0;
       if (!have && p.server) {
         have = serve_claim_root(W, &t) ? 1 : 0;
-      } else if (!have && *(volatile long long*)&ctl->next_root < nroots) {
-        atomicAdd(&ctl->pending, 1ULL);
-        long long r = (long long)atomicAdd((unsigned long long*)&ctl->next_root, 1ULL);
-        if (r < nroots) {
-          int gi = graph_of_position(root_prefix, p.n_graphs, r);
-          const DevGraph& gg = graphs[gi];
-          long long k = r - root_prefix[gi];
-          t.v[0] = gg.root_end - 1 - (int)(gg.root_offset + k * gg.root_stride);
-          t.v[1] = t.v[2] = t.v[3] = -1;
-          t.graph = gi;
-          t.part = t.parts = t.pad = 0;
-          have = 1;
-        } else {
-          atomicAdd(&ctl->pending, (unsigned long long)-1LL);
+      } else if (!have) {
+        // A big warp first takes the roots no other warp has room for.
+        if (kTiers && big && *(volatile long long*)&ctl->next_big < (long long)p.n_big_roots) {
+          atomicAdd(&ctl->pending, 1ULL);
+          long long b = (long long)atomicAdd((unsigned long long*)&ctl->next_big, 1ULL);
+          if (b < (long long)p.n_big_roots) {
+            t.v[0] = p.big_roots[b];
+            t.v[1] = t.v[2] = t.v[3] = -1;
+            t.graph = 0;
+            t.part = t.parts = t.pad = 0;
+            have = 1;
+          } else {
+            atomicAdd(&ctl->pending, (unsigned long long)-1LL);
+          }
+        }
+        if (!have && *(volatile long long*)&ctl->next_root < nroots) {
+          atomicAdd(&ctl->pending, 1ULL);
+          // Claims positions until one is not a listed big root (at most
+          // every remaining position).
+          while (true) {
+            long long r = (long long)atomicAdd((unsigned long long*)&ctl->next_root, 1ULL);
+            if (r >= nroots) {
+              atomicAdd(&ctl->pending, (unsigned long long)-1LL);
+              break;
+            }
+            int gi = graph_of_position(root_prefix, p.n_graphs, r);
+            const DevGraph& gg = graphs[gi];
+            long long k = r - root_prefix[gi];
+            const int v = gg.root_end - 1 - (int)(gg.root_offset + k * gg.root_stride);
+            if (kTiers && p.big_flag[v]) continue;
+            t.v[0] = v;
+            t.v[1] = t.v[2] = t.v[3] = -1;
+            t.graph = gi;
+            t.part = t.parts = t.pad = 0;
+            have = 1;
+            break;
+          }
         }
       }
     }
@@ -1942,6 +1978,8 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
           finished = 2;
       } else {
         finished = (*(volatile long long*)&ctl->next_root >= nroots &&
+                    (!kTiers ||
+                     *(volatile long long*)&ctl->next_big >= (long long)p.n_big_roots) &&
                     *(volatile unsigned long long*)&ctl->pending == 0ULL)
                        ? 1
                        : 0;
@@ -2003,6 +2041,24 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
       exit_ns[gridDim.x + blockIdx.x] = blk_busy;
     }
   }
+}
+
+__global__ void __launch_bounds__(kEnumThreads, 1)
+    mbe_enum_kernel(const DevGraph* graphs, const long long* root_prefix,
+                    unsigned long long* gres, const __grid_constant__ EnumParams p,
+                    const __grid_constant__ ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
+                    unsigned long long* q_seq, SlotPool pool, int32_t* scratch,
+                    unsigned long long* exit_ns) {
+  enum_main<false>(graphs, root_prefix, gres, p, sl, ctl, q_tasks, q_seq, pool, scratch, exit_ns);
+}
+
+__global__ void __launch_bounds__(kEnumThreads, 1)
+    mbe_enum_kernel_tiers(const DevGraph* graphs, const long long* root_prefix,
+                          unsigned long long* gres, const __grid_constant__ EnumParams p,
+                          const __grid_constant__ ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
+                          unsigned long long* q_seq, SlotPool pool, int32_t* scratch,
+                          unsigned long long* exit_ns) {
+  enum_main<true>(graphs, root_prefix, gres, p, sl, ctl, q_tasks, q_seq, pool, scratch, exit_ns);
 }
 
 }  // namespace gmbe

@@ -19,8 +19,19 @@ __global__ void mbe_enum_kernel(const DevGraph* graphs, const long long* root_pr
                                 const __grid_constant__ ScratchLayout sl, EnumCtl* ctl,
                                 Task* q_tasks, unsigned long long* q_seq, SlotPool pool,
                                 int32_t* scratch, unsigned long long* exit_ns);
+// The same launch with two scratch tiers (p.n_big_warps > 0): the first
+// n_big_warps warps use p.big_sl and take p.big_roots first.
+__global__ void mbe_enum_kernel_tiers(const DevGraph* graphs, const long long* root_prefix,
+                                      unsigned long long* gres,
+                                      const __grid_constant__ EnumParams p,
+                                      const __grid_constant__ ScratchLayout sl, EnumCtl* ctl,
+                                      Task* q_tasks, unsigned long long* q_seq, SlotPool pool,
+                                      int32_t* scratch, unsigned long long* exit_ns);
 
 constexpr int kSlotWordsHost = 32768;  // int32 words per sub-problem slot (128 KiB)
+// Most candidate records one slot carries (K = 1): a warp that may run
+// another warp's exported sub-problem needs room for this many candidates.
+constexpr int32_t kSlotMaxRecords = 8064;
 // Largest first-touch bitmap per warp (kEnumWarps of them fit the 227 KiB a block may use).
 constexpr int kSeenMaxWords = 3584;
 // Dynamic shared memory of a launch with layout sl.

@@ -110,6 +110,14 @@ typedef struct mbe_params {
   int32_t eager_share;     /* split_mode 0: a child of the counts tier (|L| > bitmap_max_l) */
                            /*   that passes the split test is shared out even while no  */
                            /*   warp waits: 1 = yes, <= 0 = no (default)                */
+  int32_t big_two_hop;     /* mbe_enumerate with two scratch tiers: roots whose two-hop   */
+                           /*   multiset (sum of their neighbours' degrees) exceeds this  */
+                           /*   run on a pool of warps sized for the largest root; the    */
+                           /*   other warps are sized for this bound.  0 = two tiers only */
+                           /*   when one layout for every warp does not fit the device    */
+                           /*   (the bound is then chosen); needs split_mode 0, and turns */
+                           /*   root_split_size and range_split_work off                  */
+  int32_t big_warps;       /* warps of that pool (0 = as many as fit, at most half)      */
 } mbe_params;
 
 typedef struct mbe_result {
