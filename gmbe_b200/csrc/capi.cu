@@ -504,11 +504,9 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t re, int32_t si, 
   const size_t reserve = ((size_t)2 << 30) + total_b / 50;
   const size_t avail = free_b + reusable_bytes;
   const size_t budget = avail > reserve ? avail - reserve : 0;
-  const ScratchLayout full = make_layout(nV, spec->capC, spec->capL, spec->capS);
-  const size_t full_bytes = (size_t)full.words_per_warp * sizeof(int32_t);
+  size_t full_bytes =
+      (size_t)make_layout(nV, spec->capC, spec->capL, spec->capS).words_per_warp * sizeof(int32_t);
   if (prm.big_two_hop <= 0 && full_bytes * (size_t)warps <= budget) return MBE_OK;
-  if (prm.split_mode == 1)
-    return set_error(MBE_ERR_INVALID, "split_mode 1 needs one scratch tier for every warp");
 
   // Two-hop multiset and degree of every root of this launch.
   int rc = ensure_host_csr(g);
@@ -526,6 +524,22 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t re, int32_t si, 
     S[(size_t)k] = s;
     D[(size_t)k] = h.row_off[v + 1] - h.row_off[v];
   }
+  // Capacities of this launch's roots only: a root range or shard of a large
+  // graph may fit one tier although its worst root overall does not.  Tasks
+  // below a root (its children and exported sub-problems) never need more.
+  if (n_roots > 0) {
+    const int64_t s_max = *std::max_element(S.begin(), S.end());
+    if (s_max > INT32_MAX / 2)
+      return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
+    spec->capS = (int32_t)std::max<int64_t>(s_max, 1);
+    spec->capL = std::max(*std::max_element(D.begin(), D.end()), 1);
+    spec->capC = std::max<int32_t>(1, std::min<int32_t>(nV, spec->capS));
+    full_bytes = (size_t)make_layout(nV, spec->capC, spec->capL, spec->capS).words_per_warp *
+                 sizeof(int32_t);
+    if (prm.big_two_hop <= 0 && full_bytes * (size_t)warps <= budget) return MBE_OK;
+  }
+  if (prm.split_mode == 1)
+    return set_error(MBE_ERR_INVALID, "split_mode 1 needs one scratch tier for every warp");
   // The small tier must hold any exported sub-problem a big warp makes.
   const int32_t min_c = std::min<int32_t>(spec->capC, kSlotMaxRecords);
   auto small_layout = [&](int64_t T) {
