@@ -486,8 +486,8 @@ namespace {
 // roots whose two-hop multiset is at most T, and spec->n_big warps sized for
 // the largest root, which take the listed roots (this launch's roots above T,
 // in claim order).  flags[v] marks a listed root.
-int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t re, int32_t si, int32_t sc,
-                   int32_t n_roots, size_t reusable_bytes, LaunchSpec* spec,
+int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t rb, int32_t re, int32_t si,
+                   int32_t sc, int32_t n_roots, size_t reusable_bytes, LaunchSpec* spec,
                    std::vector<int32_t>* list, std::vector<uint8_t>* flags) {
   const HostGraph& h0 = g->h;
   const int32_t nV = std::max<int32_t>(h0.V_size, 1);
@@ -506,7 +506,14 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t re, int32_t si, 
   const size_t budget = avail > reserve ? avail - reserve : 0;
   size_t full_bytes =
       (size_t)make_layout(nV, spec->capC, spec->capL, spec->capS).words_per_warp * sizeof(int32_t);
-  if (prm.big_two_hop <= 0 && full_bytes * (size_t)warps <= budget) return MBE_OK;
+  // An explicit root range is sized from its own roots below; the whole graph
+  // (and its shards) keeps the graph's capacities while they fit.
+  const bool sub_range = rb > 0 || re < h0.V_size;
+  if (!sub_range && prm.big_two_hop <= 0 && full_bytes * (size_t)warps <= budget) return MBE_OK;
+  if (n_roots == 0) {  // nothing to enumerate: the smallest layout
+    spec->capC = spec->capL = spec->capS = 1;
+    return MBE_OK;
+  }
 
   // Two-hop multiset and degree of every root of this launch.
   int rc = ensure_host_csr(g);
@@ -651,7 +658,7 @@ static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* o
   spec.n_graphs = 1;
   std::vector<int32_t> big_list;
   std::vector<uint8_t> big_flags;
-  if ((rc = plan_two_tiers(g, prm, re, si, sc, n_roots, ws.scratch_bytes, &spec, &big_list,
+  if ((rc = plan_two_tiers(g, prm, rb, re, si, sc, n_roots, ws.scratch_bytes, &spec, &big_list,
                            &big_flags)))
     return rc;
   LaunchPlan plan;
