@@ -341,3 +341,16 @@ def test_sharded_ranks_sum_to_the_whole_graph():
     # each share alone is a strict part of the whole
     half = oracle.gmbe_strided(*graph, 0, 2)
     assert 0 < half.count < want.count
+
+
+def test_large_range_fixture_reproduces(gm):
+    # The large configuration's parity fixtures (tests/golden/large_ranges.json)
+    # come from the oracle on this generator's graph: regenerate it and the
+    # cheapest range.
+    with open(os.path.join(ROOT, "tests", "golden", "large_ranges.json")) as f:
+        d = json.load(f)
+    g = gm.config_graph("large")
+    assert _digest(g.row_off, g.col) == d["csr_sha256_16"]
+    rg = d["ranges"][0]
+    o = oracle.gmbe_range(g.row_off, g.col, g.nU, rg["root_begin"], rg["root_end"], uvtrans=1)
+    assert (o.count, f"{o.set_hash:#018x}") == (rg["count"], rg["set_hash"])
