@@ -12,6 +12,8 @@ for p in (ROOT, os.path.join(ROOT, "oracle")):
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built engine")
     config.addinivalue_line("markers", "slow: long-running CPU test")
+    config.addinivalue_line("markers", "last: run after every unmarked test (new paths go last, "
+                                       "so that a stop at the first failure keeps the rest)")
 
 
 def _has_gpu():
@@ -23,6 +25,7 @@ def _has_gpu():
 
 
 def pytest_collection_modifyitems(config, items):
+    items.sort(key=lambda it: 1 if it.get_closest_marker("last") else 0)  # stable sort
     if _has_gpu():
         return
     skip = pytest.mark.skip(reason="no CUDA GPU in this environment")

@@ -14,7 +14,7 @@ import pytest
 import oracle
 from util import hub_graph, planted, random_bipartite
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.last]
 WAIT = 30 * 10**9
 
 

@@ -14,7 +14,7 @@ import os
 import numpy as np
 import pytest
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.last]
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "large_ranges.json")
 
 
