@@ -489,14 +489,23 @@ def main():
                          "algorithmic_bytes_per_launch": alg,
                          "kernel": "mbe_enum_kernel"},
         }
+        # A leg that fails is reported in the line; the measured steps stand.
         if world == 1 and not args.no_extras:
-            line["batched"] = batched_leg()
+            try:
+                line["batched"] = batched_leg()
+            except Exception as e:  # noqa: BLE001
+                log(f"batched leg failed: {e}")
+                line["batched"] = {"error": f"{type(e).__name__}: {e}"}
             line["serving"] = serving_leg_isolated()
         if world == 1 and not args.no_cpu_baseline:
             log("CPU baseline")
-            v, sample, cores = cpu_sample(g)
-            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                                    "sample": sample}
+            try:
+                v, sample, cores = cpu_sample(g)
+                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                        "sample": sample}
+            except Exception as e:  # noqa: BLE001
+                log(f"CPU baseline failed: {e}")
+                line["cpu_baseline"] = {"error": f"{type(e).__name__}: {e}"}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
