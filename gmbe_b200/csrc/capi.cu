@@ -10,6 +10,7 @@
 #include <mutex>
 
 #include "engine.h"
+#include "tiers.h"
 
 using namespace gmbe;
 
@@ -178,6 +179,83 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   s.seen_words = seen <= kSeenMaxWords ? (int32_t)seen : 0;
   return s;
 }
+
+int choose_tiers(int32_t nV, int32_t n_roots, const int64_t* S, const int32_t* D,
+                 const int32_t* roots, int warps, uint64_t budget, int64_t force_bound,
+                 int32_t force_big, TierChoice* out, std::vector<int32_t>* list,
+                 std::vector<uint8_t>* flags) {
+  *out = TierChoice();
+  list->clear();
+  flags->clear();
+  nV = std::max<int32_t>(nV, 1);
+  auto bytes_of = [&](const TierCaps& c) {
+    return (uint64_t)make_layout(nV, c.capC, c.capL, c.capS).words_per_warp * sizeof(int32_t);
+  };
+  // The launch's own capacities: tasks below a root (its children and
+  // exported sub-problems) never need more than the root.
+  TierCaps full;
+  int64_t s_max = 1;
+  for (int32_t k = 0; k < n_roots; ++k) {
+    s_max = std::max(s_max, S[k]);
+    full.capL = std::max(full.capL, D[k]);
+  }
+  if (s_max > INT32_MAX / 2)
+    return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
+  full.capS = (int32_t)s_max;
+  full.capC = std::max<int32_t>(1, std::min<int32_t>(nV, full.capS));
+  const uint64_t full_b = bytes_of(full);
+  out->small = out->big = full;
+  out->small_bytes = out->big_bytes = full_b;
+  if (force_bound <= 0 && full_b * (uint64_t)warps <= budget) return MBE_OK;
+
+  // The small tier must hold any exported sub-problem a big warp makes.
+  const int32_t min_c = std::min<int32_t>(full.capC, kSlotMaxRecords);
+  auto small_caps = [&](int64_t T) {
+    TierCaps c;
+    for (int32_t k = 0; k < n_roots; ++k)
+      if (S[k] <= T) c.capL = std::max(c.capL, D[k]);
+    c.capS = (int32_t)std::max<int64_t>(1, std::min<int64_t>(T, full.capS));
+    c.capC = std::max(min_c, std::max<int32_t>(1, std::min<int32_t>(nV, c.capS)));
+    c.capL = std::min(c.capL, full.capL);
+    return c;
+  };
+  int64_t T = force_bound;
+  if (T <= 0) {
+    T = (int64_t)1 << 16;
+    for (int64_t t = T; t < full.capS; t <<= 1)
+      if (bytes_of(small_caps(t)) * (uint64_t)warps <= budget / 10 * 6) T = t;
+  }
+  flags->assign((size_t)nV, 0);
+  for (int32_t k = 0; k < n_roots; ++k)
+    if (S[k] > T) {
+      list->push_back(roots[k]);
+      (*flags)[(size_t)roots[k]] = 1;
+    }
+  if (list->empty()) {  // every root fits the bound: one tier as usual
+    flags->clear();
+    return MBE_OK;
+  }
+  const TierCaps small = small_caps(T);
+  const uint64_t small_b = bytes_of(small);
+  if (small_b * (uint64_t)warps > budget)
+    return set_error(MBE_ERR_NOMEM, "scratch of %d warps at two-hop bound %lld: %.2f GB of %.2f GB",
+                     warps, (long long)T, small_b * (double)warps / 1e9, budget / 1e9);
+  const uint64_t extra = full_b > small_b ? full_b - small_b : 0;
+  const int64_t fit = extra ? (int64_t)((budget - small_b * (uint64_t)warps) / extra) : warps;
+  int64_t n_big = force_big > 0
+                      ? force_big
+                      : std::min<int64_t>({(int64_t)list->size(), fit, (int64_t)warps / 2});
+  n_big = std::min<int64_t>(n_big, warps);
+  if (n_big < 1 || n_big > fit)
+    return set_error(MBE_ERR_NOMEM, "%lld warps for the largest roots (%.2f GB each) do not fit",
+                     (long long)std::max<int64_t>(n_big, 1), full_b / 1e9);
+  out->n_big = (int32_t)n_big;
+  out->bound = T;
+  out->small = small;
+  out->small_bytes = small_b;
+  return MBE_OK;
+}
+
 
 int apply_tuning(const mbe_params& prm, DevGraph* dg) {
   int t2 = prm.bitmap_max_l;
@@ -479,18 +557,17 @@ int mbe_graph_free(mbe_graph* g) {
   return MBE_OK;
 }
 
+
 namespace {
 
-// Whether one scratch layout for every warp fits the device, and if not (or
-// when prm.big_two_hop asks for it) the two tiers: small warps sized for
-// roots whose two-hop multiset is at most T, and spec->n_big warps sized for
-// the largest root, which take the listed roots (this launch's roots above T,
-// in claim order).  flags[v] marks a listed root.
+// The scratch plan of one single-graph launch (see choose_tiers): the whole
+// graph with the graph's capacities while one layout for every warp fits the
+// device (no per-root pass); otherwise, and for explicit root ranges, sized
+// from this launch's roots, in two tiers where one does not fit.
 int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t rb, int32_t re, int32_t si,
                    int32_t sc, int32_t n_roots, size_t reusable_bytes, LaunchSpec* spec,
                    std::vector<int32_t>* list, std::vector<uint8_t>* flags) {
-  const HostGraph& h0 = g->h;
-  const int32_t nV = std::max<int32_t>(h0.V_size, 1);
+  const int32_t nV = std::max<int32_t>(g->h.V_size, 1);
   int dev_sms = 0, occ = 0;
   CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
@@ -504,23 +581,20 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t rb, int32_t re, 
   const size_t reserve = ((size_t)2 << 30) + total_b / 50;
   const size_t avail = free_b + reusable_bytes;
   const size_t budget = avail > reserve ? avail - reserve : 0;
-  size_t full_bytes =
+  const size_t graph_b =
       (size_t)make_layout(nV, spec->capC, spec->capL, spec->capS).words_per_warp * sizeof(int32_t);
-  // An explicit root range is sized from its own roots below; the whole graph
-  // (and its shards) keeps the graph's capacities while they fit.
-  const bool sub_range = rb > 0 || re < h0.V_size;
-  if (!sub_range && prm.big_two_hop <= 0 && full_bytes * (size_t)warps <= budget) return MBE_OK;
+  const bool sub_range = rb > 0 || re < g->h.V_size;
+  if (!sub_range && prm.big_two_hop <= 0 && graph_b * (size_t)warps <= budget) return MBE_OK;
   if (n_roots == 0) {  // nothing to enumerate: the smallest layout
     spec->capC = spec->capL = spec->capS = 1;
     return MBE_OK;
   }
-
   // Two-hop multiset and degree of every root of this launch.
   int rc = ensure_host_csr(g);
   if (rc) return rc;
   const HostGraph& h = g->h;
   std::vector<int64_t> S((size_t)n_roots);
-  std::vector<int32_t> D((size_t)n_roots);
+  std::vector<int32_t> D((size_t)n_roots), roots((size_t)n_roots);
   for (int32_t k = 0; k < n_roots; ++k) {
     const int32_t v = re - 1 - (si + k * sc);
     int64_t s = 0;
@@ -530,76 +604,21 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t rb, int32_t re, 
     }
     S[(size_t)k] = s;
     D[(size_t)k] = h.row_off[v + 1] - h.row_off[v];
+    roots[(size_t)k] = v;
   }
-  // Capacities of this launch's roots only: a root range or shard of a large
-  // graph may fit one tier although its worst root overall does not.  Tasks
-  // below a root (its children and exported sub-problems) never need more.
-  if (n_roots > 0) {
-    const int64_t s_max = *std::max_element(S.begin(), S.end());
-    if (s_max > INT32_MAX / 2)
-      return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
-    spec->capS = (int32_t)std::max<int64_t>(s_max, 1);
-    spec->capL = std::max(*std::max_element(D.begin(), D.end()), 1);
-    spec->capC = std::max<int32_t>(1, std::min<int32_t>(nV, spec->capS));
-    full_bytes = (size_t)make_layout(nV, spec->capC, spec->capL, spec->capS).words_per_warp *
-                 sizeof(int32_t);
-    if (prm.big_two_hop <= 0 && full_bytes * (size_t)warps <= budget) return MBE_OK;
-  }
-  if (prm.split_mode == 1)
+  TierChoice ch;
+  if ((rc = choose_tiers(nV, n_roots, S.data(), D.data(), roots.data(), warps, budget,
+                         prm.big_two_hop, prm.big_warps, &ch, list, flags)))
+    return rc;
+  if (ch.n_big > 0 && prm.split_mode == 1)
     return set_error(MBE_ERR_INVALID, "split_mode 1 needs one scratch tier for every warp");
-  // The small tier must hold any exported sub-problem a big warp makes.
-  const int32_t min_c = std::min<int32_t>(spec->capC, kSlotMaxRecords);
-  auto small_layout = [&](int64_t T) {
-    int32_t capL = 1;
-    for (int32_t k = 0; k < n_roots; ++k)
-      if (S[(size_t)k] <= T) capL = std::max(capL, D[(size_t)k]);
-    const int32_t capS = (int32_t)std::max<int64_t>(1, std::min<int64_t>(T, spec->capS));
-    const int32_t capC = std::max(min_c, std::max<int32_t>(1, std::min<int32_t>(nV, capS)));
-    return make_layout(nV, capC, std::min(capL, spec->capL), capS);
-  };
-  int64_t T = prm.big_two_hop;
-  if (T <= 0) {
-    // The largest power of two from 2^16 whose small tier leaves 40 % of the
-    // budget to the big warps.
-    T = (int64_t)1 << 16;
-    for (int64_t t = T; t < spec->capS; t <<= 1)
-      if ((size_t)small_layout(t).words_per_warp * sizeof(int32_t) * (size_t)warps <=
-          budget / 10 * 6)
-        T = t;
-  }
-  list->clear();
-  flags->assign((size_t)nV, 0);
-  for (int32_t k = 0; k < n_roots; ++k)
-    if (S[(size_t)k] > T) {
-      const int32_t v = re - 1 - (si + k * sc);
-      list->push_back(v);
-      (*flags)[(size_t)v] = 1;
-    }
-  if (list->empty()) {  // every root fits the small bound: one tier as usual
-    flags->clear();
-    return MBE_OK;
-  }
-  const ScratchLayout small = small_layout(T);
-  const size_t small_b = (size_t)small.words_per_warp * sizeof(int32_t);
-  if (small_b * (size_t)warps > budget)
-    return set_error(MBE_ERR_NOMEM, "scratch of %d warps at two-hop bound %lld: %.2f GB of %.2f GB",
-                     warps, (long long)T, small_b * (double)warps / 1e9, budget / 1e9);
-  const size_t extra = full_bytes > small_b ? full_bytes - small_b : 0;
-  const int64_t fit = extra ? (int64_t)((budget - small_b * (size_t)warps) / extra) : warps;
-  int64_t n_big = prm.big_warps > 0
-                      ? prm.big_warps
-                      : std::min<int64_t>({(int64_t)list->size(), fit, (int64_t)warps / 2});
-  n_big = std::min<int64_t>(n_big, warps);
-  if (n_big < 1 || n_big > fit)
-    return set_error(MBE_ERR_NOMEM, "%lld warps for the largest roots (%.2f GB each) do not fit",
-                     (long long)std::max<int64_t>(n_big, 1), full_bytes / 1e9);
-  spec->n_big = (int32_t)n_big;
-  spec->bigC = spec->capC;
-  spec->bigL = spec->capL;
-  spec->bigS = spec->capS;
-  spec->capC = small.capC;
-  spec->capL = small.capL;
-  spec->capS = small.capS;
+  spec->capC = ch.small.capC;
+  spec->capL = ch.small.capL;
+  spec->capS = ch.small.capS;
+  spec->n_big = ch.n_big;
+  spec->bigC = ch.big.capC;
+  spec->bigL = ch.big.capL;
+  spec->bigS = ch.big.capS;
   return MBE_OK;
 }
 

@@ -41,9 +41,9 @@ def digest(ro, co):
     return h.hexdigest()[:16]
 
 
-def internal_two_hop(ro, co, nU):
+def internal_two_hop(ro, co, nU, degrees=False):
     """Two-hop multiset size of every internal root, in the oracle's internal
-    order (-t 1 -o 1)."""
+    order (-t 1 -o 1), and with degrees=True each root's degree as well."""
     ro = np.ascontiguousarray(ro, np.int32)
     co = np.ascontiguousarray(co, np.int32)
     nV = len(ro) - 1
@@ -56,9 +56,14 @@ def internal_two_hop(ro, co, nU):
     du = np.bincount(co, minlength=nU).astype(np.int64)
     if n_int.value == nV:  # V rows stay the roots
         s = np.add.reduceat(du[co], ro[:-1].astype(np.int64))
+        d = dv
     else:  # -t swapped the sides: U vertices are the roots
         s = np.bincount(co, weights=dv[np.repeat(np.arange(nV), dv)], minlength=nU)
-    return s.astype(np.int64)[v_orig[: n_int.value]], n_int.value
+        d = du
+    order = v_orig[: n_int.value]
+    if degrees:
+        return s.astype(np.int64)[order], d.astype(np.int32)[order], n_int.value
+    return s.astype(np.int64)[order], n_int.value
 
 
 def main():

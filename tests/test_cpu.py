@@ -343,14 +343,126 @@ def test_sharded_ranks_sum_to_the_whole_graph():
     assert 0 < half.count < want.count
 
 
-def test_large_range_fixture_reproduces(gm):
+@pytest.fixture(scope="module")
+def large_graph(gm):
+    return gm.config_graph("large")
+
+
+def test_large_range_fixture_reproduces(gm, large_graph):
     # The large configuration's parity fixtures (tests/golden/large_ranges.json)
     # come from the oracle on this generator's graph: regenerate it and the
     # cheapest range.
     with open(os.path.join(ROOT, "tests", "golden", "large_ranges.json")) as f:
         d = json.load(f)
-    g = gm.config_graph("large")
+    g = large_graph
     assert _digest(g.row_off, g.col) == d["csr_sha256_16"]
     rg = d["ranges"][0]
     o = oracle.gmbe_range(g.row_off, g.col, g.nU, rg["root_begin"], rg["root_end"], uvtrans=1)
     assert (o.count, f"{o.set_hash:#018x}") == (rg["count"], rg["set_hash"])
+
+
+# ---------------------------------------------------------------------------
+# Scratch-tier plan (gmbe::choose_tiers, through a probe linked to the
+# library; host arithmetic only).
+
+MBE_ERR_NOMEM, MBE_ERR_CAPACITY = -5, -8
+
+
+@pytest.fixture(scope="module")
+def tiers(gm, tmp_path_factory):
+    d = tmp_path_factory.mktemp("tiers")
+    exe = d / "tiers_probe"
+    libdir = os.path.dirname(gm.LIB_PATH)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "gmbe_b200", "csrc"),
+                    "-o", str(exe), os.path.join(ROOT, "tests", "probes", "tiers_probe.cpp"),
+                    "-L", libdir, "-lgmbe", f"-Wl,-rpath,{libdir}"], check=True)
+
+    def run(nV, S, D, roots, warps=2368, budget=1 << 50, force_bound=0, force_big=0):
+        S, D, roots = (np.asarray(S, np.int64), np.asarray(D, np.int32),
+                       np.asarray(roots, np.int32))
+        req = d / "req.bin"
+        with open(req, "wb") as f:
+            f.write(np.array([nV, len(S), warps, force_big], np.int32).tobytes())
+            f.write(np.array([budget], np.uint64).tobytes())
+            f.write(np.array([force_bound], np.int64).tobytes())
+            f.write(S.tobytes() + D.tobytes() + roots.tobytes())
+        out = subprocess.run([str(exe), str(req)], check=True, capture_output=True,
+                             text=True).stdout
+        r = {}
+        for line in out.splitlines():
+            k, *v = line.split()
+            r[k] = [int(x) for x in v] if len(v) > 1 else int(v[0])
+        return r
+    return run
+
+
+def _roots(seed, n=500):
+    rng = np.random.default_rng(seed)
+    S = rng.integers(1, 20000, n)
+    D = np.minimum(S, rng.integers(1, 300, n))
+    return S, D, np.arange(n)[::-1]  # claim order: the top of the order first
+
+
+def test_tiers_one_tier_when_it_fits(tiers):
+    r = tiers(1000, [10, 50, 200], [2, 5, 9], [2, 1, 0])
+    assert (r["rc"], r["n_big"], r["list"]) == (0, 0, 0)
+    assert r["small"] == r["big"] == [200, 9, 200]  # |C| <= min(|V|, two-hop)
+
+
+def test_tiers_forced_bound_lists_the_roots_above_it(tiers):
+    S, D, roots = _roots(1)
+    r = tiers(600, S, D, roots, force_bound=5000)
+    above = S > 5000
+    assert r["rc"] == 0 and r["mismatch"] == 0
+    assert r["list"] == r["flagged"] == above.sum()
+    assert r["first"] == roots[np.argmax(above)]
+    assert r["last"] == roots[len(S) - 1 - np.argmax(above[::-1])]
+    assert r["n_big"] == min(above.sum(), 2368 // 2) and r["bound"] == 5000
+    assert r["big"] == [min(600, S.max()), D.max(), S.max()]
+    # the small tier: the bound, the degrees below it, and room for any
+    # exported sub-problem of a big warp (8,064 records)
+    assert r["small"] == [max(min(min(600, S.max()), 8064), min(600, 5000)), D[~above].max(), 5000]
+
+
+def test_tiers_forced_pool_and_bound_above_every_root(tiers):
+    S, D, roots = _roots(2)
+    assert tiers(600, S, D, roots, force_bound=1000, force_big=3)["n_big"] == 3
+    r = tiers(600, S, D, roots, force_bound=int(S.max()))
+    assert (r["rc"], r["n_big"], r["list"], r["flagged"]) == (0, 0, 0, 0)
+
+
+def test_tiers_report_what_does_not_fit(tiers):
+    S, D, roots = _roots(3)
+    assert tiers(600, S, D, roots, budget=4096, force_bound=1000)["rc"] == MBE_ERR_NOMEM
+    big = tiers(600, S, D, roots, force_bound=1000)
+    # room for the small tier and less than one big warp more
+    budget = big["small_bytes"] * 2368 + (big["big_bytes"] - big["small_bytes"]) // 2
+    assert tiers(600, S, D, roots, budget=budget, force_bound=1000)["rc"] == MBE_ERR_NOMEM
+    assert tiers(600, [1 << 31], [5], [0])["rc"] == MBE_ERR_CAPACITY
+
+
+def test_tiers_plan_of_the_large_configuration(tiers, large_graph):
+    # The whole large graph on 148 x 16 warps with 185 GB for scratch: one
+    # layout for the worst root does not fit, so two tiers are planned.
+    sys_path = os.path.join(ROOT, "tests", "golden")
+    import sys
+    if sys_path not in sys.path:
+        sys.path.insert(0, sys_path)
+    from make_large_ranges import internal_two_hop
+    g = large_graph
+    S, D, n = internal_two_hop(g.row_off, g.col, g.nU, degrees=True)
+    roots = np.arange(n)[::-1]
+    warps, budget = 148 * 16, 185 * 10**9
+    r = tiers(n, S[roots], D[roots], roots, warps=warps, budget=budget)
+    assert r["rc"] == 0 and r["mismatch"] == 0 and r["n_big"] >= 1
+    T = r["bound"]
+    assert T >= 1 << 16 and T & (T - 1) == 0
+    assert r["small_bytes"] * warps <= budget * 6 // 10
+    assert r["list"] == (S > T).sum() == r["flagged"]
+    fit = (budget - r["small_bytes"] * warps) // (r["big_bytes"] - r["small_bytes"])
+    assert r["n_big"] == min(r["list"], fit, warps // 2)
+    total = r["small_bytes"] * (warps - r["n_big"]) + r["big_bytes"] * r["n_big"]
+    assert total <= budget
+    print(f"large plan: bound {T}, {r['list']} listed roots, {r['n_big']} big warps, "
+          f"small {r['small_bytes'] / 1e6:.1f} MB, big {r['big_bytes'] / 1e9:.3f} GB, "
+          f"total {total / 1e9:.1f} GB")
