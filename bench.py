@@ -23,6 +23,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -67,12 +68,12 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix=f"gmbe_clocks{self.index}_", suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader",
                  "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
@@ -88,9 +89,12 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.f.close()
+        with open(self.path) as f:
+            lines = f.readlines()
+        os.unlink(self.path)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -187,22 +191,6 @@ def run_profile_case():
         raise SystemExit("profile case not reproducible")
     print(json.dumps({"profile_case": "medium, 16 blocks, roots p = 0 mod 64", "count": b.count,
                       "set_hash": f"{b.set_hash:#x}", "kernel_ms": b.kernel_ms}), flush=True)
-
-
-def run_profile_full():
-    """The bench's own launch for one-pass ncu metrics (DRAM bytes): the whole
-    medium graph with the default parameters, one warm-up and one profiled
-    enumeration, both checked against the known count and set hash."""
-    import gmbe_b200 as gm
-    consts = load_consts()
-    g = gm.config_graph(WORKLOAD)
-    with gm.Graph.from_csr(g.row_off, g.col, g.nU, **FLAGS) as G:
-        rs = [G.enumerate() for _ in range(2)]
-    for r in rs:
-        if (r.count, f"{r.set_hash:#x}") != (consts["count"], consts["set_hash"]):
-            raise SystemExit(f"full launch mismatch: {r.count} {r.set_hash:#x}")
-    print(json.dumps({"profile_case": "medium, full launch", "count": rs[1].count,
-                      "set_hash": f"{rs[1].set_hash:#x}", "kernel_ms": rs[1].kernel_ms}), flush=True)
 
 
 def batched_leg(n=4096, replays=3, plain_stride=4):
@@ -347,8 +335,6 @@ def main():
                     help="skip the batched and serving legs (they run at N=1 only)")
     ap.add_argument("--profile", action="store_true",
                     help="one reduced launch for ncu: 16 blocks, every 64th root (~1.6 GB scratch)")
-    ap.add_argument("--profile-full", action="store_true",
-                    help="the full medium launch for one-pass ncu metrics (DRAM bytes)")
     ap.add_argument("--serving-leg", action="store_true",
                     help="run only the serving leg and print its result (used by the N=1 run)")
     args = ap.parse_args()
@@ -357,9 +343,6 @@ def main():
         return
     if args.profile:
         run_profile_case()
-        return
-    if args.profile_full:
-        run_profile_full()
         return
     if args.serving_leg:
         print(json.dumps(serving_leg()), flush=True)

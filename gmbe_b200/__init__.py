@@ -61,7 +61,8 @@ class Params(C.Structure):
                 ("root_split_size", C.c_int32), ("share_min_work", C.c_int32),
                 ("range_split_work", C.c_int32), ("range_chunk", C.c_int32),
                 ("eager_share", C.c_int32), ("big_two_hop", C.c_int32),
-                ("big_warps", C.c_int32)]
+                ("big_warps", C.c_int32), ("reserved_p", C.c_int32),
+                ("time_limit_ns", C.c_int64)]
 
 
 class Result(C.Structure):

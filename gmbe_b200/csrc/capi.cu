@@ -231,8 +231,13 @@ int choose_tiers(int32_t nV, int32_t n_roots, const int64_t* S, const int32_t* D
       list->push_back(roots[k]);
       (*flags)[(size_t)roots[k]] = 1;
     }
-  if (list->empty()) {  // every root fits the bound: one tier as usual
+  if (list->empty()) {  // every root fits the bound: one tier, if it fits at all
     flags->clear();
+    if (force_bound <= 0 && full_b * (uint64_t)warps > budget)
+      return set_error(MBE_ERR_NOMEM,
+                       "scratch of %d warps: %.2f GB of %.2f GB, and no root is above the "
+                       "two-hop bound %lld that a second tier would take",
+                       warps, full_b * (double)warps / 1e9, budget / 1e9, (long long)T);
     return MBE_OK;
   }
   const TierCaps small = small_caps(T);
@@ -361,6 +366,7 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.queue_cap = qcap;
   ep.slot_spin_limit = 20000000;  // x ~64 ns sleeps: a claimed slot is written within microseconds
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
+  ep.time_limit_ns = std::max<int64_t>(prm.time_limit_ns, 0);
   ep.record_exit = prm.sm_timing ? 1 : 0;
   ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
   // Heavy roots split into vertex tuples (sub-problem sharing mode only).
@@ -432,6 +438,8 @@ int engine_status(Workspace& ws, const EnumCtl& ctl) {
       return set_error(MBE_ERR_TIMEOUT, "split-queue slot %llu was never written", ctl.err_info);
     case kStCapacity:
       return set_error(MBE_ERR_CAPACITY, "scratch capacity exceeded (info 0x%llx)", ctl.err_info);
+    case kStDeadline:
+      return set_error(MBE_ERR_TIMEOUT, "launch time limit reached (result incomplete)");
     default:
       return set_error(MBE_ERR_CUDA, "device status %d", ctl.status);
   }

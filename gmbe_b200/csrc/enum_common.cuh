@@ -11,6 +11,7 @@ enum : int32_t {
   kStTimeout = 1,    // a bounded wait ran out
   kStQueue = 2,      // queue slot never became valid
   kStCapacity = 3,   // a scratch bound was exceeded
+  kStDeadline = 4,   // the launch's time limit ran out
 };
 
 // Graph in HBM (internal numbering).  rev_* is the U -> V transpose.
@@ -146,6 +147,7 @@ struct EnumParams {
   int32_t queue_cap;
   int64_t slot_spin_limit;    // iterations waiting for a claimed slot to be written
   int64_t idle_ns_limit;      // nanoseconds a warp may idle waiting for work
+  int64_t time_limit_ns;      // > 0: the launch gives up after this long (kStDeadline)
   int32_t record_exit;        // -p
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)

@@ -45,6 +45,24 @@ __device__ void set_status(EnumCtl* ctl, int32_t code, unsigned long long info) 
   atomicExch(&ctl->abort, 1);
 }
 
+// Whether this warp should leave its task (lane-uniform): the launch is
+// aborting, or its time limit has passed (which starts the abort).
+template <typename WarpT>
+__device__ __forceinline__ bool must_stop(const WarpT& W) {
+  int s = 0;
+  if (lane_id() == 0) {
+    s = *(volatile int32_t*)&W.ctl->abort;
+    if (!s && W.deadline != 0) {
+      const uint64_t now = globaltimer_ns();
+      if (now > W.deadline) {
+        set_status(W.ctl, kStDeadline, now - W.deadline);
+        s = 1;
+      }
+    }
+  }
+  return __shfl_sync(0xffffffffu, s, 0) != 0;
+}
+
 // Visits every entry of a list of rows with all 32 lanes busy.  row_of(r, beg,
 // len) describes row r; visit(valid, r, pos) is called by every lane (uniform
 // control flow), pos indexing the global entry array.
@@ -94,6 +112,7 @@ struct Warp {
   unsigned long long shape;        // last task set up: |C| | (part << 32) | (parts << 48)
   unsigned long long ns_t1;        // time inside the counts tier (bitmap tier excluded)
   uint32_t* seen;                  // this warp's first-touch bitmap in shared memory, or null
+  uint64_t deadline;               // %globaltimer after which the launch gives up (0: never)
 
   __device__ int32_t* A(int64_t off) const { return base + off; }
   __device__ uint64_t* A64(int64_t off) const { return reinterpret_cast<uint64_t*>(base + off); }
@@ -431,7 +450,9 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
   }
   __syncwarp();
   int level = 1;
+  unsigned steps = 0;
   while (level != 0) {
+    if ((++steps & 4095u) == 0u && must_stop(W)) return;
     uint32_t* R = reinterpret_cast<uint32_t*>(lrec[level - 1]);
     const int n = ln[level - 1];
     uint32_t Lm[K];
@@ -1078,8 +1099,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
   __syncwarp();
   int level = 1;
   while (level != 0) {
-    int ab = lane == 0 ? *(volatile int32_t*)&W.ctl->abort : 0;
-    if (__shfl_sync(kFull, ab, 0)) return;
+    if (must_stop(W)) return;
     int cur = -1;
     const int end = level == 1 ? t.nend : t.nC;  // the first level may push a part only
     for (int b0 = stack[level - 1]; b0 < end; b0 += 32) {
@@ -1861,6 +1881,7 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
   W.cnt = W.hash = W.nonmax = W.splits = 0;
   W.ns_t1 = W.ns_t2 = W.n_t2 = 0;
   W.pushes = W.shape = 0;
+  W.deadline = p.time_limit_ns > 0 ? t_start + (uint64_t)p.time_limit_ns : 0;
   uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0, max_split = 0;
   uint64_t max_pushes = 0, max_shape = 0;
   int32_t max_gid = 0;
@@ -1869,11 +1890,8 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
   uint64_t busy_ns = 0, last_done_ns = 0, idle_last = 0;
   while (true) {
     int ab = 0;
-    if (lane == 0) {
-      ab = *(volatile int32_t*)&ctl->abort;
-      if (p.server) ab |= *(volatile int32_t*)&p.serve.sctl->stop;  // server shutting down
-    }
-    if (__shfl_sync(kFull, ab, 0)) break;
+    if (lane == 0 && p.server) ab = *(volatile int32_t*)&p.serve.sctl->stop;  // shutting down
+    if (__shfl_sync(kFull, ab, 0) || must_stop(W)) break;
     Task t;
     int have = 0;
     if (lane == 0) {

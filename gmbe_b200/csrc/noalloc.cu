@@ -216,6 +216,7 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   ep.queue_cap = kNoAllocQueueCap;
   ep.slot_spin_limit = 20000000;
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
+  ep.time_limit_ns = prm.time_limit_ns > 0 ? prm.time_limit_ns : 0;
   ep.record_exit = 0;
   SlotPool none;
   none.slots = nullptr;

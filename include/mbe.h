@@ -118,6 +118,11 @@ typedef struct mbe_params {
                            /*   (the bound is then chosen); needs split_mode 0, and turns */
                            /*   root_split_size and range_split_work off                  */
   int32_t big_warps;       /* warps of that pool (0 = as many as fit, at most half)      */
+  int32_t reserved_p;      /* zero */
+  int64_t time_limit_ns;   /* a launch that runs longer than this gives up: every warp    */
+                           /*   leaves at its next check (task boundary, counts-tier step,*/
+                           /*   or every 4,096 bitmap-tier steps) and the call returns    */
+                           /*   MBE_ERR_TIMEOUT; the result is then incomplete.  0 = none */
 } mbe_params;
 
 typedef struct mbe_result {
@@ -220,8 +225,12 @@ const char* mbe_last_error_string(void);
  *   d_rev_off[nU+1], d_rev_col[nE] its transpose (U -> V rows, ascending)
  *   max_two_hop   optional bound on sum_{u in N(v)} d(u) over all roots v
  *                 (0 = use nE); a tighter bound lets more warps fit the pool
- *   params        NULL = defaults; sm_timing, queue_capacity, root range and
- *                 shards are ignored (all roots, fixed 4096-entry split ring)
+ *   params        NULL = defaults; sm_timing, queue_capacity, root range,
+ *                 shards, split_mode, direct_max_c and the sharing settings
+ *                 are ignored: all roots, a fixed 4096-entry split ring, GMBE's
+ *                 vertex-tuple children (split_mode 1, as there is no room for
+ *                 sub-problem slots), and every task whose |L| fits the bitmap
+ *                 tier goes there straight from set-up
  * Output (device memory, owned by the caller): d_out[4] = count, set hash,
  * non-maximal branches, device status (0 = OK, else a device error code).
  * Ids in the hash are the input ids.

@@ -439,6 +439,11 @@ def test_tiers_report_what_does_not_fit(tiers):
     budget = big["small_bytes"] * 2368 + (big["big_bytes"] - big["small_bytes"]) // 2
     assert tiers(600, S, D, roots, budget=budget, force_bound=1000)["rc"] == MBE_ERR_NOMEM
     assert tiers(600, [1 << 31], [5], [0])["rc"] == MBE_ERR_CAPACITY
+    # Every root below the smallest two-hop bound, yet one layout for every
+    # warp (the count map over 10^7 vertices is 40 MB a warp) is above the
+    # budget: a second tier cannot help, and the plan says so.
+    r = tiers(10**7, [900, 1000], [3, 4], [1, 0], budget=10 * 10**9)
+    assert (r["rc"], r["n_big"], r["list"]) == (MBE_ERR_NOMEM, 0, 0)
 
 
 def test_tiers_plan_of_the_large_configuration(tiers, large_graph):

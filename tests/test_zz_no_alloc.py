@@ -8,15 +8,17 @@ buffers owned by the test (the caller) and check that, on two calls in a
 row, it returns exactly what the allocating entry point mbe_enumerate returns
 for the same graph (count and set hash are integers: the tolerance is zero).
 
-The file name sorts last so that a run stopping at the first failure has run
-every other test before this one.
+The file name sorts last among the test files and its tests carry the `last`
+marker, which the conftest's ordering puts after every unmarked test; among
+the `last` tests collection order holds, so a run that stops at the first
+failure has run every other test before these.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.last]
 
 
 def _lib(gm):
