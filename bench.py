@@ -193,44 +193,52 @@ def run_profile_case():
                       "set_hash": f"{b.set_hash:#x}", "kernel_ms": b.kernel_ms}), flush=True)
 
 
-def batched_leg(n=4096, replays=3, plain_stride=4):
+BATCH_ORACLE = os.path.join(ROOT, "tests", "golden", "batch_oracle.json")
+
+
+def batched_leg(n=4096, replays=3):
     """Batched workload: n graphs of the batched distribution (seeds 1000..)
     in one persistent launch replayed from a CUDA graph, against one plain
-    launch per graph on every plain_stride-th graph (graphs resident on the
-    device in both arms); per-graph results must be equal."""
+    launch per graph over all n graphs (graphs resident on the device in
+    both arms).  Every per-graph count and set hash of every replay is
+    compared with the plain launches and with the CPU oracle's values
+    (tests/golden/batch_oracle.json)."""
     import gmbe_b200 as gm
+    with open(BATCH_ORACLE) as f:
+        orc = json.load(f)
+    want = list(zip(orc["count"], (int(h, 16) for h in orc["set_hash"])))[:n]
     log("batched: generating")
     gs = [gm.batch_graph(1000 + i) for i in range(n)]
     log("batched: building")
     B = gm.Batch(gs)
     per, tot = B.run()  # capture + warm-up
+    equal_oracle = [(r.count, r.set_hash) for r in per] == want
     walls = []
     for _ in range(replays):
         t = time.perf_counter()
         per, tot = B.run()
         walls.append(time.perf_counter() - t)
+        equal_oracle &= [(r.count, r.set_hash) for r in per] == want
     wall = statistics.median(walls)
+    B.free()
     log("batched: plain arm")
-    sample = list(range(0, n, plain_stride))
-    Gs = [gm.Graph.from_csr(gs[i].row_off, gs[i].col, gs[i].nU, **FLAGS) for i in sample]
+    Gs = [gm.Graph.from_csr(g.row_off, g.col, g.nU, **FLAGS) for g in gs]
     Gs[0].enumerate()
     t = time.perf_counter()
     plain = [G.enumerate() for G in Gs]
     plain_wall = time.perf_counter() - t
-    equal = all((plain[k].count, plain[k].set_hash) == (per[i].count, per[i].set_hash)
-                for k, i in enumerate(sample))
+    equal_plain = [(r.count, r.set_hash) for r in plain] == [(r.count, r.set_hash) for r in per]
     for G in Gs:
         G.free()
-    B.free()
     return {"graphs": n, "graphs_per_s": n / wall, "replay_ms": wall * 1e3,
             "kernel_ms": tot.kernel_ms, "bicliques": tot.count,
-            "plain_graphs_per_s": len(sample) / plain_wall,
-            "plain_sample": f"every {plain_stride}th graph, one mbe_enumerate each",
-            "speedup_vs_plain": (n / wall) / (len(sample) / plain_wall),
-            "results_equal_plain": equal}
+            "plain_graphs_per_s": n / plain_wall,
+            "plain_sample": f"all {n} graphs, one mbe_enumerate each",
+            "speedup_vs_plain": (n / wall) / (n / plain_wall),
+            "results_equal_plain": equal_plain, "results_equal_oracle": equal_oracle}
 
 
-def serving_leg(n=1000, rates=(1000, 5000, 20000)):
+def serving_leg(n=1000, rates=(100, 200, 300, 1000, 5000, 20000)):
     """Serving: n requests (95 % batched-distribution graphs, 5 % medium
     serving graphs; stream seed 7) submitted at Poisson arrival times for each
     offered load, through mbe_server_*; latency from arrival to result.  The

@@ -1,21 +1,33 @@
 """The benchmark workloads as seeded generator specs.
 
-Each configuration is a Chung-Lu bipartite graph (see ``mbe_gen_chung_lu`` in
-include/mbe.h) with the shape the workload names.  All of them cap the
-probability of any single (u, v) pair at 0.1: with hub weights whose product
-exceeds the edge count, plain Chung-Lu saturates a block of hubs to a
-near-complete bipartite graph, and the few missing edges of such a block give
-2^k maximal bicliques for k hubs (measured: the top roots of the uncapped
-medium graph hold 1, 2, 4, ..., 128 bicliques each), which no enumerator can
-finish.  The cap keeps every marginal named by the workload (sizes, edge
-count, exponents, degree caps as expected-degree caps) and removes only that
-saturation.
+The specs live in workloads.json beside this file (one source for this module
+and for the stand-alone mbe_gen program, which the timed CPU runs of the
+reference's own enumerators use to make the same inputs without loading the
+engine).  Each configuration is a Chung-Lu bipartite graph (see
+``mbe_gen_chung_lu`` in include/mbe.h) with the shape the workload names.
+All of them cap the probability of any single (u, v) pair at 0.1: with hub
+weights whose product exceeds the edge count, plain Chung-Lu saturates a
+block of hubs to a near-complete bipartite graph, and the few missing edges
+of such a block give 2^k maximal bicliques for k hubs (measured: the top
+roots of the uncapped medium graph hold 1, 2, 4, ..., 128 bicliques each),
+which no enumerator can finish.  The cap keeps every marginal named by the
+workload (sizes, edge count, exponents, degree caps as expected-degree caps)
+and removes only that saturation.
 """
 from __future__ import annotations
 
+import json
+import os
+
 from . import GenSpec, batch_spec, generate
 
+WORKLOADS_JSON = os.path.join(os.path.dirname(os.path.abspath(__file__)), "workloads.json")
+
+with open(WORKLOADS_JSON) as _f:
+    _W = json.load(_f)
+
 PAIR_P_MAX = 0.1
+FIELDS = _W["fields"]
 
 
 def _spec(nU, nV, nE, gu, gv, mu, mv, seed, n_blocks=0, bu=0, bv=0, bp=0.0):
@@ -24,26 +36,19 @@ def _spec(nU, nV, nE, gu, gv, mu, mv, seed, n_blocks=0, bu=0, bv=0, bp=0.0):
                    reserved=0, block_p=bp, pair_p_max=PAIR_P_MAX)
 
 
-CONFIGS = {
-    # small: 2,000 x 3,000, ~20,000 edges, exponent 2.1 both sides, degree cap 200
-    "small": lambda: _spec(2000, 3000, 20000, 2.1, 2.1, 200, 200, 1),
-    # medium skewed: 100,000 x 400,000, ~2,000,000 edges, exponents 2.0 / 2.4,
-    # degree cap 5,000, plus 64 planted 24 x 24 blocks at edge probability 0.7
-    "medium": lambda: _spec(100000, 400000, 2000000, 2.0, 2.4, 5000, 5000, 2, 64, 24, 24, 0.7),
-    # large: 2,000,000 x 8,000,000, ~60,000,000 edges, exponents 2.1 / 2.2, cap 50,000
-    "large": lambda: _spec(2000000, 8000000, 60000000, 2.1, 2.2, 50000, 50000, 3),
-    # serving mix, medium requests: 20,000 x 80,000, ~300,000 edges, exponent 2.1
-    "serve_medium": lambda: _spec(20000, 80000, 300000, 2.1, 2.1, 2000, 2000, 7),
-}
+def _from_json(d):
+    return GenSpec(reserved=0, **d)
+
+
+# small: 2,000 x 3,000, ~20,000 edges, exponent 2.1 both sides, degree cap 200
+# medium skewed: 100,000 x 400,000, ~2,000,000 edges, exponents 2.0 / 2.4,
+#   degree cap 5,000, plus 64 planted 24 x 24 blocks at edge probability 0.7
+# large: 2,000,000 x 8,000,000, ~60,000,000 edges, exponents 2.1 / 2.2, cap 50,000
+# serving mix, medium requests: 20,000 x 80,000, ~300,000 edges, exponent 2.1
+CONFIGS = {name: (lambda d=w["spec"]: _from_json(d)) for name, w in _W["workloads"].items()}
 
 # Workload names as the benchmark reports them.
-DESCRIPTIONS = {
-    "small": "MBE 2k x 3k Chung-Lu (gamma 2.1/2.1, cap 200, seed 1, ~20k edges)",
-    "medium": ("MBE 100k x 400k Chung-Lu (gamma 2.0/2.4, cap 5000, seed 2, ~2M edges) "
-               "+ 64 planted 24x24 blocks p=0.7"),
-    "large": "MBE 2M x 8M Chung-Lu (gamma 2.1/2.2, cap 50000, seed 3, ~60M edges)",
-    "serve_medium": "MBE 20k x 80k Chung-Lu (gamma 2.1, cap 2000, ~300k edges)",
-}
+DESCRIPTIONS = {name: w["description"] for name, w in _W["workloads"].items()}
 
 
 def config_graph(name: str):
@@ -69,4 +74,3 @@ def serve_mix(n: int, seed: int = 7, medium_share: float = 0.05, medium_pool: in
     is_med = rng.random(n) < medium_share
     graphs = [med[i % medium_pool] if is_med[i] else batch_graph(1000 + i) for i in range(n)]
     return graphs, is_med
-

@@ -56,7 +56,7 @@ struct EnumCtl {
   int32_t status;        // first error code
   int32_t abort;         // set together with status
   int32_t idle_warps;    // warps waiting for work (export demand)
-  int32_t pad0;
+  int32_t closing;       // serving: the launch is ending (no new roots are claimed)
   unsigned long long pending;   // queued + running tasks (termination)
   unsigned long long q_head;    // next slot to consume
   unsigned long long q_tail;    // next slot to produce

@@ -1801,6 +1801,8 @@ __device__ bool serve_claim_root(Warp& W, Task* t) {
   const ServeLink& L = W.p.serve;
   volatile ServeCtl* sc = L.sctl;
   if (sc->arr_head >= sc->arr_tail) return false;
+  // A launch that is ending takes no new roots: the host relaunches for them.
+  if (*(volatile int32_t*)&W.ctl->closing) return false;
   atomicAdd(&W.ctl->pending, 1ULL);
   for (int tries = 0; tries < 64; ++tries) {
     const unsigned long long h = sc->arr_head;
@@ -1987,12 +1989,19 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
       continue;
     }
     // 1: leave now; 2 (serving): nothing in flight and no published roots left.
+    // A serving launch ends as a whole: the first warp to see it quiet for
+    // idle_exit_ns sets `closing`, after which no warp claims a new root and
+    // every warp leaves once nothing is pending.  Graphs published meanwhile
+    // wait for the host's next launch, which gets the whole grid.  (Warps
+    // that left one by one would let arrivals keep a launch of a few
+    // remaining warps alive indefinitely.)
     int finished = 0;
     if (lane == 0) {
       if (p.server) {
         volatile ServeCtl* sc = p.serve.sctl;
-        if (sc->stop) finished = 1;
-        else if (*(volatile unsigned long long*)&ctl->pending == 0ULL && sc->arr_head >= sc->arr_tail)
+        const bool quiet = *(volatile unsigned long long*)&ctl->pending == 0ULL;
+        if (sc->stop || (quiet && *(volatile int32_t*)&ctl->closing)) finished = 1;
+        else if (quiet && sc->arr_head >= sc->arr_tail)
           finished = 2;
       } else {
         finished = (*(volatile long long*)&ctl->next_root >= nroots &&
@@ -2014,7 +2023,10 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
     } else if (p.server && finished == 2 && now - idle_since > (uint64_t)p.serve.idle_exit_ns) {
       // A serving launch ends once it has had nothing to do for a while; the
       // host launches again when graphs arrive.
-      if (lane == 0) atomicSub(&ctl->idle_warps, 1);
+      if (lane == 0) {
+        atomicExch(&ctl->closing, 1);
+        atomicSub(&ctl->idle_warps, 1);
+      }
       break;
     } else if (now - idle_since > (uint64_t)p.idle_ns_limit) {
       if (lane == 0) set_status(ctl, kStTimeout, now - idle_since);

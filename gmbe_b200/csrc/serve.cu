@@ -247,10 +247,14 @@ void fail_all(mbe_server* s, int rc) {
   s->resident = 0;
 }
 
-// Copies one admitted graph into the arena and publishes it (server thread).
-// The copies are from pageable memory: each call returns once its source is
-// staged, so the image may be dropped right after.
-int admit(mbe_server* s, Request* r) {
+// Copies one admitted graph into the arena and publishes it (server thread,
+// which holds s->mu on entry and on return).  The arena space, the arrival
+// ring position and the request's state are taken under the lock; the copies
+// themselves run with the lock released, so that submit, poll and wait are
+// never held up behind a graph's staging copy.  The image moves out of the
+// request first: nothing another thread does to the request (destroy
+// finishing it) touches the memory being copied.
+int admit(mbe_server* s, Request* r, std::unique_lock<std::mutex>& lk) {
   const size_t off = s->bump;
   char* base = s->d_arena + off;
   DevGraph& g = r->dg;
@@ -265,23 +269,30 @@ int admit(mbe_server* s, Request* r) {
   hdr.g = g;
   hdr.pending = (unsigned long long)g.n_roots;
   hdr.request = r->id;
-  memcpy(r->image.data(), &hdr, sizeof(hdr));
-  SCK(cudaMemcpyAsync(base, r->image.data(), r->bytes, cudaMemcpyHostToDevice, s->s_copy));
-  const uint32_t blk = (uint32_t)(off >> kServeBlockShift);
-  SCK(cudaMemcpyAsync(s->d_arr_blk + (s->published % (uint64_t)s->arr_cap), &blk, sizeof(blk),
-                      cudaMemcpyHostToDevice, s->s_copy));
-  const unsigned long long tail = s->published + 1;
-  SCK(cudaMemcpyAsync(&s->d_sctl->arr_tail, &tail, sizeof(tail), cudaMemcpyHostToDevice,
-                      s->s_copy));
-  SCK(cudaEventRecord(s->ev_copy, s->s_copy));
+  std::vector<char> image = std::move(r->image);
+  r->image = std::vector<char>();
+  memcpy(image.data(), &hdr, sizeof(hdr));
+  const size_t bytes = r->bytes;
+  const uint64_t slot = s->published % (uint64_t)s->arr_cap;
   r->arena_off = off;
-  s->bump = off + r->bytes;
+  s->bump = off + bytes;
   s->published++;
   s->resident++;
   s->st.admitted++;
   r->state = kResident;
-  r->image.clear();
-  r->image.shrink_to_fit();
+  const uint32_t blk = (uint32_t)(off >> kServeBlockShift);
+  const unsigned long long tail = s->published;
+  lk.unlock();
+  cudaError_t e = cudaMemcpyAsync(base, image.data(), bytes, cudaMemcpyHostToDevice, s->s_copy);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_arr_blk + slot, &blk, sizeof(blk), cudaMemcpyHostToDevice, s->s_copy);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&s->d_sctl->arr_tail, &tail, sizeof(tail), cudaMemcpyHostToDevice,
+                        s->s_copy);
+  if (e == cudaSuccess) e = cudaEventRecord(s->ev_copy, s->s_copy);
+  lk.lock();
+  if (e != cudaSuccess)
+    return set_error(MBE_ERR_CUDA, "copying a graph to the device: %s", cudaGetErrorString(e));
   return MBE_OK;
 }
 
@@ -332,12 +343,15 @@ void server_loop(mbe_server* s) {
       Request* r = s->waiting.front();
       if (s->resident >= s->cfg.max_graphs) break;
       if (s->bump + r->bytes > (size_t)s->cfg.arena_bytes) break;  // rewinds once drained
-      int rc = admit(s, r);
       s->waiting.pop_front();
+      const uint64_t id = r->id;
+      int rc = admit(s, r, lk);
       if (rc) {
         s->fatal = rc;
         s->fatal_msg = "copying a graph to the device failed";
-        finish(s, r, rc);
+        // The lock was released during the copy: look the request up again.
+        auto it = s->reqs.find(id);
+        if (it != s->reqs.end() && it->second->state == kResident) finish(s, it->second, rc);
         fail_all(s, rc);
         break;
       }
