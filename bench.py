@@ -1,21 +1,28 @@
 #!/usr/bin/env python
-"""Benchmark: maximal-biclique enumeration of the medium skewed workload.
+"""Benchmark: maximal-biclique enumeration of the large workload.
 
-One step = one complete enumeration of the medium graph (100k x 400k Chung-Lu,
-~2M edges, 64 planted 24x24 blocks; seeded, synthetic) through the engine,
-with the reference's flags -t 1 -o 1 -f and bounds 20/1500.  The graph is
+Workload: the large configuration, a 2M x 8M Chung-Lu bipartite graph (~60M
+edges, exponents 2.1/2.2, expected-degree cap 50,000, seed 3; synthetic),
+with the reference's flags -t 1 -o 1 -f and bounds 20/1500.  The whole graph
+holds about 12 billion maximal bicliques, far more than one timed step can
+enumerate, so one step is one launch over one interleaved root shard: step i
+enumerates the roots at positions p = i mod S (S = 512 by default) of the
+internal degree order, about 1/512 of the graph.  Shards sample every part of
+the degree order alike, the heaviest roots at the top included.  The graph is
 resident in HBM before the timed region; every step's count and set hash are
-checked against the recorded oracle values.
+checked against the shard pins in tests/golden/large_bench_shards.json.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun: each rank enumerates an interleaved share of the
-roots (shard_index = rank) and one NCCL all-reduce sums (count, set hash) per
-step; value = the graph's bicliques / the slowest rank's device time.
+N > 1 runs under torchrun: at step i rank r enumerates shard i*N + r, so the
+work per GPU is fixed as N grows (weak scaling), with no data-path
+collective; value = all ranks' bicliques / the slowest rank's device time.
 
---impl reference times the CPU restatement of the same path (oracle/, the
-GMBE per-root DFS with OpenMP over every host core) on a stratified sample of
-the roots, because the reference has no CPU implementation of its GPU path.
+Extra legs at N = 1: the medium configuration (whole graph per launch, its
+count and hash pinned by the oracle), the 4,096-graph batched workload, the
+serving workload, and the CPU baseline.  --impl reference times the
+reference's own CPU enumerator (MbeaFinderBitset, built from the reference's
+sources into oracle/_ref/) on the same root sample the CPU baseline uses.
 """
 import argparse
 import json
@@ -30,11 +37,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-WORKLOAD = "medium"
+WORKLOAD = "large"
 METRIC = "maximal bicliques/s"
 UNIT = "bicliques/s"
 FLAGS = dict(uvtrans=1, order=1, fast_mode=1)
 CONSTS = os.path.join(ROOT, "gmbe_b200", "workload_constants.json")
+WORKLOADS = os.path.join(ROOT, "gmbe_b200", "workloads.json")
+SHARD_PINS = os.path.join(ROOT, "tests", "golden", "large_bench_shards.json")
+LARGE_ORACLE = os.path.join(ROOT, "tests", "golden", "large_shards.json")
+SHARDS = 512
 FALLBACK_HBM_GBS = 6650.0
 _T0 = time.time()
 
@@ -44,9 +55,16 @@ def log(msg):
     print(f"[bench {time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
-def load_consts():
+def load_consts(name):
     with open(CONSTS) as f:
-        return json.load(f)[WORKLOAD]
+        return json.load(f)[name]
+
+
+def load_json(path):
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
 
 
 def peaks():
@@ -111,65 +129,88 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(g, target_s=10.0):
-    """Oracle (CPU port of the path, all host cores) on a stratified root
-    sample sized to ~target_s; returns (bicliques/s, description, cores)."""
-    import oracle
+REF_SAMPLER = os.path.join(ROOT, "oracle", "_ref", "ref_mbea")
+MBE_GEN = os.path.join(ROOT, "gmbe_b200", "mbe_gen")
+# The CPU sample: one root in CPU_STRIDE from the lowest CPU_MAX_ROOT of the
+# reference's root order (its MbeaFinderBitset costs seconds to minutes per
+# root above that, so a bounded sample cannot include them; leaving them out
+# overstates the CPU rate, the higher roots having far fewer bicliques per
+# second).
+CPU_STRIDE = 4000
+CPU_MAX_ROOT = 0.8
+
+
+def write_workload_adj(name, path):
+    """Writes a workload's .adj with the stand-alone generator (no engine)."""
+    w = load_json(WORKLOADS)
+    spec = w["workloads"][name]["spec"]
+    subprocess.run([MBE_GEN, path] + [str(spec[f]) for f in w["fields"]], check=True,
+                   stdout=subprocess.DEVNULL)
+
+
+def ref_samples(adj, first, count, threads, stride=CPU_STRIDE, max_root=CPU_MAX_ROOT):
+    """The reference's own CPU enumerator (MbeaFinderBitset, src/BicliqueFinder.cu:
+    59-197, built from its sources into oracle/_ref/ref_mbea) on root samples
+    first .. first+count-1 of a workload: sample j = roots j, j + stride, ...
+    of the lowest max_root of its root order, on `threads` OpenMP threads.
+    The graph is read once (untimed); returns [(bicliques, seconds), ...]."""
+    if not os.path.exists(REF_SAMPLER):
+        raise FileNotFoundError("oracle/_ref/ref_mbea is not built")
+    p = subprocess.run([REF_SAMPLER, adj, "2", "1", "1", str(stride), str(first), str(count),
+                        str(threads), str(max_root)], check=True, capture_output=True, text=True)
+    out = []
+    for line in p.stdout.splitlines():
+        f = line.split()
+        if f and f[0] == "sample":
+            out.append((int(f[5]), float(f[7])))
+    if len(out) != count:
+        raise RuntimeError(f"reference sampler printed {len(out)} of {count} samples")
+    return out
+
+
+def sample_text(name, first, count):
+    return (f"reference MbeaFinderBitset (oracle/_ref, built from the reference's sources) on "
+            f"root samples {first}..{first + count - 1} of the {name} workload: sample j = "
+            f"every {CPU_STRIDE}th root from j of the lowest {CPU_MAX_ROOT:.0%} of its root "
+            f"order (higher roots take seconds to minutes each on the CPU); OpenMP over roots; "
+            f"graph read excluded")
+
+
+def cpu_baseline_leg(warmup, steps):
+    """The same samples the reference arm times at this --steps/--warmup."""
     cores = os.cpu_count() or 1
-    t = time.perf_counter()
-    oracle.gmbe_strided(g.row_off, g.col, g.nU, 1 << 30, 1, threads=cores)  # graph set-up only
-    t_setup = time.perf_counter() - t
-    stride = 512
-    while True:
-        t = time.perf_counter()
-        r = oracle.gmbe_strided(g.row_off, g.col, g.nU, 0, stride, threads=cores)
-        dt = max(time.perf_counter() - t - t_setup, 1e-6)
-        if dt >= target_s / 4 or stride == 1:
-            break
-        stride = max(1, stride // 4)
-    return r.count / dt, f"every {stride}th root of the {WORKLOAD} graph from the top of the " \
-                         f"degree order: {r.count} bicliques in {dt:.2f} s (graph set-up excluded)", cores
+    with tempfile.TemporaryDirectory() as d:
+        adj = os.path.join(d, f"{WORKLOAD}.adj")
+        write_workload_adj(WORKLOAD, adj)
+        res = ref_samples(adj, warmup, steps, cores)
+    cnt = sum(c for c, _ in res)
+    sec = sum(t for _, t in res)
+    return {"value": cnt / sec, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": sample_text(WORKLOAD, warmup, steps) + f": {cnt} bicliques in {sec:.2f} s"}
 
 
 def run_reference(args):
-    """The reference arm: CPU restatement of the path on all host cores."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    """The reference arm: the reference's own CPU enumerator on all host
+    cores, timed per step on one root sample of the workload (warm-up steps
+    are the first samples).  Loads nothing from the engine: the workload's
+    .adj comes from the stand-alone generator.  Rank 0 alone runs."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    import gmbe_b200 as gm
-    import oracle
-    g = gm.config_graph(WORKLOAD)
     cores = os.cpu_count() or 1
-    t = time.perf_counter()
-    oracle.gmbe_strided(g.row_off, g.col, g.nU, 1 << 30, 1, threads=cores)
-    t_setup = time.perf_counter() - t
-    # Sample size: ~20 s for the whole run.
-    stride = 256
-    t = time.perf_counter()
-    oracle.gmbe_strided(g.row_off, g.col, g.nU, 0, stride, threads=cores)
-    per = max(time.perf_counter() - t - t_setup, 1e-3)
-    budget = 20.0 / max(1, args.steps + args.warmup)
-    while per * 2 < budget and stride > 1:
-        stride //= 2
-        per *= 2
-    for i in range(args.warmup):
-        oracle.gmbe_strided(g.row_off, g.col, g.nU, i % stride, stride, threads=cores)
-    tot, cnt = 0.0, 0
-    for i in range(args.steps):
-        t = time.perf_counter()
-        r = oracle.gmbe_strided(g.row_off, g.col, g.nU, i % stride, stride, threads=cores)
-        tot += max(time.perf_counter() - t - t_setup, 1e-9)
-        cnt += r.count
-    value = cnt / tot
-    sample = (f"per step every {stride}th root of the {WORKLOAD} graph (offsets 0..{args.steps - 1}), "
-              f"CPU restatement of the GMBE path, OpenMP over roots; graph set-up excluded")
+    with tempfile.TemporaryDirectory() as d:
+        adj = os.path.join(d, f"{WORKLOAD}.adj")
+        write_workload_adj(WORKLOAD, adj)
+        res = ref_samples(adj, 0, args.warmup + args.steps, cores)[args.warmup:]
+    cnt = sum(c for c, _ in res)
+    sec = sum(t for _, t in res)
+    value = cnt / sec
+    sample = sample_text(WORKLOAD, args.warmup, args.steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic", "config": {"workload": WORKLOAD_DESC(), "flags": "-t 1 -o 1 -f",
-                                        "bound_height": 20, "bound_size": 1500},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": workload_config(args.gpus),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -177,20 +218,24 @@ def run_reference(args):
 
 
 def run_profile_case():
-    """A reduced launch of the same kernel for ncu captures: 16 blocks and a
-    stratified 1/64 share of the medium graph's roots, one warm-up and one
-    profiled enumeration.  Sized so ncu's multi-pass replay stays within a
-    few GB of device memory and a minute or two."""
+    """A reduced launch of the enumeration kernel on the large graph for ncu
+    captures: 16 blocks over the roots [1000000, 1005000) of the internal
+    order (two-hop multisets up to 18,495, so the scratch is a few GB), one
+    warm-up and one profiled enumeration, both checked against the oracle's
+    count and set hash (tests/golden/large_ranges.json)."""
     import gmbe_b200 as gm
+    rg = [r for r in load_json(os.path.join(ROOT, "tests", "golden", "large_ranges.json"))["ranges"]
+          if r["root_begin"] == 1000000][0]
     g = gm.config_graph(WORKLOAD)
-    with gm.Graph.from_csr(g.row_off, g.col, g.nU, **FLAGS) as G:
-        kw = dict(blocks=16, shard_count=64, shard_index=0)
-        a = G.enumerate(**kw)
-        b = G.enumerate(**kw)
-    if (a.count, a.set_hash) != (b.count, b.set_hash):
-        raise SystemExit("profile case not reproducible")
-    print(json.dumps({"profile_case": "medium, 16 blocks, roots p = 0 mod 64", "count": b.count,
-                      "set_hash": f"{b.set_hash:#x}", "kernel_ms": b.kernel_ms}), flush=True)
+    with gm.Graph.build_on_device(g.row_off, g.col, g.nU, **FLAGS) as G:
+        kw = dict(blocks=16, root_begin=rg["root_begin"], root_end=rg["root_end"])
+        rs = [G.enumerate(**kw) for _ in range(2)]
+    for r in rs:
+        if (r.count, f"{r.set_hash:#018x}") != (rg["count"], rg["set_hash"]):
+            raise SystemExit(f"profile case mismatch: {r.count} {r.set_hash:#x}")
+    print(json.dumps({"profile_case": "large, 16 blocks, roots [1000000, 1005000)",
+                      "count": rs[1].count, "set_hash": f"{rs[1].set_hash:#x}",
+                      "kernel_ms": rs[1].kernel_ms}), flush=True)
 
 
 BATCH_ORACLE = os.path.join(ROOT, "tests", "golden", "batch_oracle.json")
@@ -327,22 +372,84 @@ def serving_leg_isolated(limit_s=SERVING_LIMIT_S):
         return {"error": "serving leg printed no result"}
 
 
-def WORKLOAD_DESC():
+def workload_config(world):
+    w = load_json(WORKLOADS)["workloads"][WORKLOAD]
+    return {"workload": w["description"], "flags": "-t 1 -o 1 -f", "bound_height": 20,
+            "bound_size": 1500,
+            "step": f"one launch over one interleaved root shard: roots at positions p = s mod "
+                    f"{SHARDS} of the internal degree order, shard s = step * n_gpus + rank",
+            "parallelism": f"{world} GPU(s), one shard each per step" if world > 1 else "1 GPU",
+            "l2": "inputs (CSR ~0.5 GB, scratch tens of GB) larger than the 126 MB L2"}
+
+
+def shard_pins():
+    d = load_json(SHARD_PINS)
+    if not d or d.get("shard_count") != SHARDS:
+        return {}
+    return {int(k): (v["count"], int(v["set_hash"], 16)) for k, v in d["shards"].items()}
+
+
+def alg_bytes_per_biclique():
+    """Algorithmic bytes (the GMBE tree's reads, counted by the oracle) per
+    maximal biclique on the large graph: from the oracle's pinned 1/20000
+    shards, which sample the whole degree order; a step's algorithmic bytes
+    are its bicliques times this."""
+    d = load_json(LARGE_ORACLE)
+    if not d:
+        return None, None
+    sh = [x for x in d["shards"] if "alg_bytes" in x]
+    if not sh:
+        return None, None
+    b = sum(x["alg_bytes"] for x in sh) / sum(x["count"] for x in sh)
+    return b, (f"{b:.0f} B per biclique: the oracle's GMBE-tree bytes over its pinned shards "
+               + ", ".join(f"{x['shard_index']}/{x['shard_count']}" for x in sh))
+
+
+def medium_leg(steps=5, warmup=2):
+    """The medium configuration, whole graph per launch (the previous
+    headline): count and hash pinned by the oracle on every launch."""
+    import torch
     import gmbe_b200 as gm
-    return gm.DESCRIPTIONS[WORKLOAD]
+    consts = load_consts("medium")
+    g = gm.config_graph("medium")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    with gm.Graph.build_on_device(g.row_off, g.col, g.nU, **FLAGS) as G:
+        for _ in range(warmup):
+            G.enumerate()
+        ms, skew, busy = [], [], []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = G.enumerate(sm_timing=1)
+            if (r.count, f"{r.set_hash:#x}") != (consts["count"], consts["set_hash"]):
+                raise RuntimeError(f"medium mismatch: {r.count} {r.set_hash:#x}")
+            ms.append(r.kernel_ms)
+            skew.append(r.sm_exit_max_ms - r.sm_exit_min_ms)
+            busy.append(r.warp_busy_frac)
+    peak, kind = peaks()
+    kern = statistics.mean(ms)
+    ach = consts["alg_bytes"] / (kern / 1e3) / 1e9
+    return {"workload": gm.DESCRIPTIONS["medium"], "bicliques_per_launch": consts["count"],
+            "value": consts["count"] / (kern / 1e3), "unit": UNIT, "kernel_ms": kern,
+            "kernel_ms_all": ms, "sm_last_task_skew_ms": statistics.median(skew),
+            "warp_busy_frac": statistics.median(busy), "results_equal_oracle": True,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_kind": kind,
+                         "algorithmic_bytes_per_launch": consts["alg_bytes"]}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the batched and serving legs (they run at N=1 only)")
+                    help="skip the medium, batched and serving legs (they run at N=1 only)")
     ap.add_argument("--profile", action="store_true",
-                    help="one reduced launch for ncu: 16 blocks, every 64th root (~1.6 GB scratch)")
+                    help="one reduced launch for ncu: 16 blocks, roots [1000000, 1005000) of the "
+                         "large graph (a few GB)")
     ap.add_argument("--serving-leg", action="store_true",
                     help="run only the serving leg and print its result (used by the N=1 run)")
     args = ap.parse_args()
@@ -356,7 +463,6 @@ def main():
         print(json.dumps(serving_leg()), flush=True)
         return
 
-    import numpy as np
     import torch
     import torch.distributed as dist
     import gmbe_b200 as gm
@@ -368,132 +474,154 @@ def main():
     dev = torch.device("cuda", local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    if args.warmup < 1 or args.steps < 1:
+        raise SystemExit("--steps and --warmup must be >= 1")
+    if (args.warmup + args.steps) * world > SHARDS:
+        raise SystemExit(f"more than {SHARDS} shards requested")
 
-    consts = load_consts()
+    log("generating the large graph")
     g = gm.config_graph(WORKLOAD)
-    G = gm.Graph.from_csr(g.row_off, g.col, g.nU, device=local, **FLAGS)
-    from gmbe_b200.dist import shard_params, sum_results
-    shard = shard_params(rank, world)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    G = gm.Graph.build_on_device(g.row_off, g.col, g.nU, device=local, **FLAGS)
+    pins = shard_pins()
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    def reduce_result(r):
-        return sum_results(r.count, r.set_hash, device=dev)
+    # Timed steps take shards 0 .. K*N-1; warm-ups the last shards.
+    def shard_of(step, timed):
+        k = step * world + rank
+        return k if timed else SHARDS - 1 - k
 
-    def check(c, h):
-        if (c, h) != (consts["count"], int(consts["set_hash"], 16)):
-            raise SystemExit(f"result mismatch: count {c} hash {h:#x}, expected "
-                             f"{consts['count']} {consts['set_hash']}")
+    checked, mismatched = [], []
 
-    for _ in range(args.warmup):
-        check(*reduce_result(G.enumerate(**shard)))
+    def check(shard, r):
+        want = pins.get(shard)
+        if want is None:
+            return
+        if (r.count, r.set_hash) != want:
+            mismatched.append(shard)
+        else:
+            checked.append(shard)
 
+    log("warm-up")
+    for i in range(args.warmup):
+        si = shard_of(i, False)
+        check(si, G.enumerate(shard_count=SHARDS, shard_index=si))
     clocks = ClockSampler(local)
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    step_ms, kern_ms, exit_skew, busy = [], [], [], []
-    for _ in range(args.steps):
-        flush.zero_()
+    step_ms, kern_ms, skew, busy, counts, results = [], [], [], [], [], []
+    log("timed steps")
+    for i in range(args.steps):
+        si = shard_of(i, True)
         torch.cuda.synchronize()
         barrier()
         ev0.record()
-        r = G.enumerate(sm_timing=1, **shard)
+        r = G.enumerate(shard_count=SHARDS, shard_index=si, sm_timing=1)
         ev1.record()
         torch.cuda.synchronize()
         barrier()
         step_ms.append(ev0.elapsed_time(ev1))
         kern_ms.append(r.kernel_ms)
-        exit_skew.append(r.sm_exit_max_ms - r.sm_exit_min_ms)
+        skew.append(r.sm_exit_max_ms - r.sm_exit_min_ms)
         busy.append(r.warp_busy_frac)
-        check(*reduce_result(r))
+        counts.append(r.count)
+        results.append({"shard": si, "count": r.count, "set_hash": f"{r.set_hash:#018x}",
+                        "kernel_ms": round(r.kernel_ms, 2)})
+        check(si, r)
     clk = clocks.stop()
-    total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
-    kern_total = torch.tensor([sum(kern_ms)], dtype=torch.float64, device=dev)
+    tot = torch.tensor([sum(step_ms), sum(kern_ms), float(sum(counts))], dtype=torch.float64,
+                       device=dev)
     if world > 1:
-        dist.all_reduce(total_ms, op=dist.ReduceOp.MAX)
-        dist.all_reduce(kern_total, op=dist.ReduceOp.MAX)
-    total_ms = float(total_ms.item())
-    kern_mean_ms = float(kern_total.item()) / args.steps
-    value = consts["count"] * args.steps / (total_ms / 1000.0)
+        t_max = tot[:2].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        n_all = tot[2:].clone()
+        dist.all_reduce(n_all, op=dist.ReduceOp.SUM)
+        tot = torch.cat([t_max, n_all])
+    total_ms, kern_total, n_bic = (float(x) for x in tot.tolist())
+    value = n_bic / (total_ms / 1e3)
 
     # ---- end to end through the public API with host buffers ----
-    log("timed steps done; end-to-end calls")
-    e2e_steps = max(1, min(args.steps, 3))
-    # Each call uploads the .adj-shaped CSR once and builds the graph on the
-    # device (mbe_graph_build_on_device), then enumerates; it reads back the
-    # build's checks (8 B), its capacities (24 B), the internal row order
-    # (4 B per internal V vertex), the launch's control block (208 B) and the
-    # result (24 B).
-    iV = min(g.nV, g.nU) if FLAGS["uvtrans"] == 1 else g.nV
-    h2d = 4 * ((g.nV + 1) + g.nE)
-    d2h = 8 + 24 + 4 * iV + 208 + 24
+    # Each call uploads the .adj-shaped CSR, builds the graph on the device
+    # (mbe_graph_build_on_device), enumerates the step's shard and reads the
+    # result back.
+    log("end-to-end calls")
     G.free()
-
-    def e2e_leg(build):
-        secs = []
-        for _ in range(e2e_steps):
-            barrier()
-            t = time.perf_counter()
-            with build(g.row_off, g.col, g.nU, device=local, **FLAGS) as G2:
-                r = G2.enumerate(**shard)
-            secs.append(time.perf_counter() - t)
-            check(*reduce_result(r))
-        tot = torch.tensor([sum(secs)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-        return consts["count"] * e2e_steps / float(tot.item())
-
-    e2e_value = e2e_leg(gm.Graph.build_on_device)
-    # The same call with the graph built on the host (mbe_graph_from_csr),
-    # which uploads the CSR, its transpose and the hash keys.
-    e2e_host_value = e2e_leg(gm.Graph.from_csr)
+    e2e_steps = max(1, min(args.steps, 3))
+    h2d = 4 * ((g.nV + 1) + g.nE)
+    iV = min(g.nV, g.nU)
+    d2h = 8 + 24 + 4 * iV + 256 + 24
+    secs, e2e_n = [], 0
+    for i in range(e2e_steps):
+        si = shard_of(i, True)
+        barrier()
+        t = time.perf_counter()
+        with gm.Graph.build_on_device(g.row_off, g.col, g.nU, device=local, **FLAGS) as G2:
+            r = G2.enumerate(shard_count=SHARDS, shard_index=si)
+        secs.append(time.perf_counter() - t)
+        e2e_n += r.count
+        check(si, r)
+    e2e = torch.tensor([sum(secs), float(e2e_n)], dtype=torch.float64, device=dev)
+    if world > 1:
+        a = e2e[:1].clone()
+        dist.all_reduce(a, op=dist.ReduceOp.MAX)
+        b = e2e[1:].clone()
+        dist.all_reduce(b, op=dist.ReduceOp.SUM)
+        e2e = torch.cat([a, b])
+    e2e_secs, e2e_bic = (float(x) for x in e2e.tolist())
+    bad = torch.tensor([len(mismatched)], device=dev)
+    if world > 1:
+        dist.all_reduce(bad)
 
     if rank == 0:
         peak, peak_kind = peaks()
-        alg = consts["alg_bytes"] / max(world, 1)
-        achieved = alg / (kern_mean_ms / 1000.0) / 1e9
+        bpb, bpb_src = alg_bytes_per_biclique()
+        kern_mean = kern_total / args.steps
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC(), "flags": "-t 1 -o 1 -f", "bound_height": 20,
-                       "bound_size": 1500, "bicliques_per_step": consts["count"],
-                       "parallelism": f"roots interleaved over {world} GPU(s)" if world > 1 else "1 GPU",
-                       "l2": "flushed (256 MB write) before every timed step"},
-            "enum_ms_per_step": kern_mean_ms,
-            "sm_last_task_skew_ms": statistics.median(exit_skew),
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": workload_config(world),
+            "bicliques_per_step": n_bic / args.steps,
+            "enum_ms_per_step": kern_mean,
+            "sm_last_task_skew_ms": statistics.median(skew),
             "warp_busy_frac": statistics.median(busy),
+            "steps_detail": results,
+            "pins": {"fixture": os.path.relpath(SHARD_PINS, ROOT), "shards_checked": len(checked),
+                     "mismatches": int(bad.item())},
             "gpu_launches": args.steps,
             "clocks": clk,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e": {"value": e2e_bic / e2e_secs, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                    "api": "mbe_graph_build_on_device + mbe_enumerate",
-                    "host_build_value": e2e_host_value},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": consts.get("traffic_bytes_per_launch"),
-                         "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg,
-                         "kernel": "mbe_enum_kernel"},
+                    "api": "mbe_graph_build_on_device + mbe_enumerate (one shard) from host arrays"},
         }
+        if bpb:
+            alg = bpb * n_bic / args.steps / world
+            ach = alg / (kern_mean / 1e3) / 1e9
+            line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                                "frac": ach / peak, "peak_kind": peak_kind,
+                                "traffic": load_consts("large").get("traffic_bytes_per_biclique", 0)
+                                * n_bic / args.steps / world or None,
+                                "algorithmic_bytes_per_launch": alg,
+                                "algorithmic_bytes_source": bpb_src,
+                                "kernel": "mbe_enum_kernel_tiers / mbe_enum_kernel"}
         # A leg that fails is reported in the line; the measured steps stand.
         if world == 1 and not args.no_extras:
-            try:
-                line["batched"] = batched_leg()
-            except Exception as e:  # noqa: BLE001
-                log(f"batched leg failed: {e}")
-                line["batched"] = {"error": f"{type(e).__name__}: {e}"}
+            for name, fn in (("medium", medium_leg), ("batched", batched_leg)):
+                log(f"{name} leg")
+                try:
+                    line[name] = fn()
+                except Exception as e:  # noqa: BLE001
+                    log(f"{name} leg failed: {e}")
+                    line[name] = {"error": f"{type(e).__name__}: {e}"}
             line["serving"] = serving_leg_isolated()
         if world == 1 and not args.no_cpu_baseline:
             log("CPU baseline")
             try:
-                v, sample, cores = cpu_sample(g)
-                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                                        "sample": sample}
+                line["cpu_baseline"] = cpu_baseline_leg(args.warmup, args.steps)
             except Exception as e:  # noqa: BLE001
                 log(f"CPU baseline failed: {e}")
                 line["cpu_baseline"] = {"error": f"{type(e).__name__}: {e}"}
@@ -501,6 +629,8 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    if int(bad.item()):
+        raise SystemExit(f"{int(bad.item())} shard results differ from the pins")
 
 
 if __name__ == "__main__":

@@ -152,7 +152,8 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   s.lp = take(Lc);
   s.aoff = take(Lc + 1);
   s.stack = take(Lc + 2);
-  s.lsize = take(Lc + 2);
+  s.lent = take(Lc + 2);
+  s.lbits = take((int64_t)kLevelBits * ((C + 31) / 32));
   s.aadj = take(S);
   s.cadj = take(S);
   s.masks = take((int64_t)(kKMax + 1) * C);  // bitmap-tier records (K+1 words each)

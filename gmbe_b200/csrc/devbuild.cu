@@ -3,14 +3,14 @@
 // the -t side swap, the -o 0/1/2 row ordering, both CSRs -- plus the hash keys
 // and the per-warp capacities, on the GPU from the uploaded .adj-shaped CSR.
 //
-// One deliberate difference from the host build: rows of equal degree keep
-// their input order, where the reference breaks such ties lexicographically.
-// The order only decides which root owns a biclique and how work is spread;
-// the set of maximal bicliques, hence the count and the set hash, does not
-// depend on it.
+// The -o order is the host build's exactly: rows by size, then by content
+// (lexicographic, as the reference's comparator, src/BiGraph.cu:75-85), then
+// by original id, so a graph built here has the same internal ids, hence the
+// same roots in every root range and shard, as one built on the host.
 //
-// Sorting uses CUB's stable radix sort (header-only, shipped with the CUDA
-// toolkit); the other steps are the kernels below.  The row offsets are
+// Sorting uses CUB (header-only, shipped with the CUDA toolkit): a merge sort
+// of row ids under that comparator for the order, stable radix sorts for the
+// transposes; the other steps are the kernels below.  The row offsets are
 // checked on the host (O(nV)) before any kernel indexes through them; the
 // entries (O(nE)) are checked on the device before anything is built from them.
 #include <cuda_runtime.h>
@@ -92,15 +92,28 @@ __global__ void k_rows_of(const int32_t* off, int32_t n, int32_t* row_of) {
     for (int32_t j = off[v] + lane; j < off[v + 1]; j += 32) row_of[j] = v;
 }
 
-// Sort key of row v: its degree (ascending) or INT32_MAX - degree (descending).
-__global__ void k_degree_keys(const int32_t* off, int32_t n, int32_t descending, int32_t* key,
-                              int32_t* ident) {
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const int32_t d = off[v + 1] - off[v];
-    key[v] = descending ? INT32_MAX - d : d;
+__global__ void k_iota(int32_t n, int32_t* ident) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
     ident[v] = v;
-  }
 }
+
+// The row order of -o 1 (ascending size) and -o 2 (descending): equal sizes
+// compare by content, lexicographically ascending, then by row id (the row's
+// original id, which makes the order total).
+struct RowOrder {
+  const int32_t* off;
+  const int32_t* adj;
+  int32_t descending;
+  __device__ bool operator()(const int32_t& a, const int32_t& b) const {
+    const int32_t sa = off[a + 1] - off[a], sb = off[b + 1] - off[b];
+    if (sa != sb) return descending ? sa > sb : sa < sb;
+    const int32_t* pa = adj + off[a];
+    const int32_t* pb = adj + off[b];
+    for (int32_t i = 0; i < sa; ++i)
+      if (pa[i] != pb[i]) return pa[i] < pb[i];
+    return a < b;
+  }
+};
 
 __global__ void k_permuted_degrees(const int32_t* off, const int32_t* perm, int32_t n, int32_t* out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -209,7 +222,7 @@ int device_build_graph(mbe_graph* g, const int32_t* row_off, const int32_t* col,
   int rc = check_offsets(row_off, nV, nE);
   if (rc) return rc;
   int32_t *d_ro = nullptr, *d_co = nullptr, *d_rowof = nullptr, *d_uoff = nullptr,
-          *d_uadj = nullptr, *d_key = nullptr, *d_keyo = nullptr, *d_ident = nullptr,
+          *d_uadj = nullptr,
           *d_perm = nullptr, *d_pdeg = nullptr, *d_flags = nullptr;
   unsigned long long* d_caps = nullptr;
   void* tmp = nullptr;
@@ -252,21 +265,18 @@ int device_build_graph(mbe_graph* g, const int32_t* row_off, const int32_t* col,
   iU = swap ? nV : nU;
   // -o: 0 keeps the input order; 1 sorts rows by degree ascending; every
   // other value descending (the reference comparator's reading under -f).
-  DCK(cudaMalloc((void**)&d_key, sizeof(int32_t) * iV));
-  DCK(cudaMalloc((void**)&d_keyo, sizeof(int32_t) * iV));
-  DCK(cudaMalloc((void**)&d_ident, sizeof(int32_t) * iV));
   DCK(cudaMalloc((void**)&d_perm, sizeof(int32_t) * iV));
   DCK(cudaMalloc((void**)&d_pdeg, sizeof(int32_t) * ((size_t)iV + 1)));
   DCK(cudaMalloc((void**)&d_caps, sizeof(caps)));
-  k_degree_keys<<<blocks_for(iV), kThreads>>>(voff, iV, o.order == 1 ? 0 : 1, d_key, d_ident);
+  k_iota<<<blocks_for(iV), kThreads>>>(iV, d_perm);
   DCK(cudaGetLastError());
-  DCK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, d_key, d_keyo, d_ident, d_perm, iV));
-  DCK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, d_pdeg, d_pdeg, iV + 1));
-  DCK(cudaMalloc(&tmp, std::max<size_t>(std::max(sort_bytes, scan_bytes), 1)));
-  if (o.order != 0)
-    DCK(cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, d_key, d_keyo, d_ident, d_perm, iV));
-  else
-    DCK(cudaMemcpy(d_perm, d_ident, sizeof(int32_t) * iV, cudaMemcpyDeviceToDevice));
+  {
+    const RowOrder cmp{voff, vadj, o.order == 1 ? 0 : 1};
+    DCK(cub::DeviceMergeSort::SortKeys(nullptr, sort_bytes, d_perm, (int64_t)iV, cmp));
+    DCK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, d_pdeg, d_pdeg, iV + 1));
+    DCK(cudaMalloc(&tmp, std::max<size_t>(std::max(sort_bytes, scan_bytes), 1)));
+    if (o.order != 0) DCK(cub::DeviceMergeSort::SortKeys(tmp, sort_bytes, d_perm, (int64_t)iV, cmp));
+  }
   k_permuted_degrees<<<blocks_for(iV), kThreads>>>(voff, d_perm, iV, d_pdeg);
   DCK(cudaGetLastError());
   DCK(cudaMemset(d_pdeg + iV, 0, sizeof(int32_t)));
@@ -316,9 +326,6 @@ done:
   cudaFree(d_rowof);
   cudaFree(d_uoff);
   cudaFree(d_uadj);
-  cudaFree(d_key);
-  cudaFree(d_keyo);
-  cudaFree(d_ident);
   cudaFree(d_perm);
   cudaFree(d_pdeg);
   cudaFree(d_flags);

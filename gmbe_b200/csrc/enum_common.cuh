@@ -82,7 +82,8 @@ struct ScratchLayout {
   int32_t capC, capL, capS, kmax;
   // offsets
   int64_t map, touched, cv, ncnt, bound, coff, fill, sidx;
-  int64_t lv, llevel, lp, aoff, stack, lsize;
+  int64_t lv, llevel, lp, aoff, stack, lent;  // lent: entries of each level's L rows
+  int64_t lbits;        // counts-tier level bitmaps (kLevelBits x ceil(capC / 32) words)
   int64_t aadj, cadj;
   int64_t masks, sub_v, tcls;  // tcls: class of each touched candidate of a sparse push
   int64_t ckey, ent;           // ckey: hash key per candidate (uint64); ent: packed entries

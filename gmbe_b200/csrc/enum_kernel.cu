@@ -785,12 +785,58 @@ __device__ __forceinline__ void t1_rows_at_level(Warp& W, const T1& t, int lvl, 
   }
 }
 
+// Selects the L positions of candidate x's row (cadj) with llevel == lvl,
+// calling fn(pos) over their rows of aadj: the rows a push of x keeps, walked
+// without a pass over all of L.
+template <typename Fn>
+__device__ __forceinline__ void t1_rows_of(Warp& W, int x, int lvl, Fn fn) {
+  const int32_t* llevel = W.A(W.sl.llevel);
+  const int32_t* aoff = W.A(W.sl.aoff);
+  const int32_t* coff = W.A(W.sl.coff);
+  const int32_t* cadj = W.A(W.sl.cadj);
+  const int lane = (int)lane_id();
+  const int rb = coff[x], re = coff[x + 1];
+  for (int c0 = rb; c0 < re; c0 += 32) {
+    const int j = c0 + lane;
+    const int l = j < re ? cadj[j] : 0;
+    const bool sel = j < re && llevel[l] == lvl;
+    const unsigned bal = __ballot_sync(kFull, sel);
+    const int nsel = __popc(bal);
+    if (nsel == 0) continue;
+    int myrow = -1;
+    {
+      unsigned m = bal;
+      for (int k = 0; k < lane && m; ++k) m &= m - 1;
+      if (lane < nsel) myrow = __shfl_sync(kFull, l, __ffs(m) - 1);
+      else __shfl_sync(kFull, l, 0);
+    }
+    flat_rows(
+        nsel,
+        [&](int, int& beg, int& len) {
+          beg = aoff[myrow];
+          len = aoff[myrow + 1] - beg;
+        },
+        fn);
+  }
+}
+
+// finder_pop (src/IterFinderGpu.h:266-303) of candidate x at `level`, walking
+// only the rows of the level above it: the removed rows (llevel == level-1)
+// restore their counts and mark the candidates they meet, and the kept rows
+// (llevel == level, the rows of x) decide the pruning.  A pass over every
+// candidate is not needed: a candidate adjacent to neither kept nor removed
+// rows has count 0 at this level and every level below it, so no push, scan,
+// maximality test or later pop at or below this level reads its bound, and
+// the pop one level up treats every bound >= level-1 alike.
 __device__ void t1_pop(Warp& W, const T1& t, int x, int level) {
   int32_t* llevel = W.A(W.sl.llevel);
   int32_t* ncnt = W.A(W.sl.ncnt);
   int32_t* bound = W.A(W.sl.bound);
   const int32_t* aadj = W.A(W.sl.aadj);
+  const int32_t* coff = W.A(W.sl.coff);
+  const int32_t* cadj = W.A(W.sl.cadj);
   const int lane = (int)lane_id();
+  const bool prune = W.p.prune != 0;
   // restore counts over L_parent \ L_child and mark touched candidates
   t1_rows_at_level(W, t, level - 1, [&](bool valid, int, int pos) {
     if (!valid) return;
@@ -800,16 +846,33 @@ __device__ void t1_pop(Warp& W, const T1& t, int x, int level) {
     if (bound[p] >= level) bound[p] = kTouched;
   });
   __syncwarp();
-  for (int l = lane; l < t.nL; l += 32)
-    if (llevel[l] >= level) llevel[l] = level - 1;
+  if (prune) {
+    // Candidates of the kept rows that no removed row met are retired at this
+    // level (a candidate in several kept rows is visited several times: the
+    // write is the same each time, and touched ones are left for the pass
+    // below).
+    t1_rows_of(W, x, level, [&](bool valid, int, int pos) {
+      if (!valid) return;
+      const int p = aadj[pos];
+      if (p < 0 || p == x) return;
+      const int b = bound[p];
+      if (b >= level && b != kTouched) bound[p] = level - 1;
+    });
+    __syncwarp();
+    // touched candidates -> free
+    t1_rows_at_level(W, t, level - 1, [&](bool valid, int, int pos) {
+      if (!valid) return;
+      const int p = aadj[pos];
+      if (p >= 0 && bound[p] == kTouched) bound[p] = kFree;
+    });
+    __syncwarp();
+  }
+  if (lane == 0) bound[x] = kFree;
   __syncwarp();
-  if (W.p.prune) {
-    for (int i = lane; i < t.nC; i += 32) {
-      int b = bound[i];
-      if (b >= level) bound[i] = (b == kTouched || i == x) ? kFree : level - 1;
-    }
-  } else {
-    if (lane == 0) bound[x] = kFree;
+  // the kept rows go back to the level above (deeper levels are popped already)
+  for (int j = coff[x] + lane; j < coff[x + 1]; j += 32) {
+    const int l = cadj[j];
+    if (llevel[l] == level) llevel[l] = level - 1;
   }
   __syncwarp();
 }
@@ -1078,44 +1141,96 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   __syncwarp();
 }
 
+// Levels 2 .. kLevelBits + 1 of the counts tier keep a bitmap of the
+// candidates the level's L meets (count != 0 there): the scan for the next
+// live candidate and a recount walk its words instead of every candidate.
+__device__ __forceinline__ uint32_t* level_bits(const Warp& W, int level) {
+  if (level < 2 || level > kLevelBits + 1) return nullptr;
+  return reinterpret_cast<uint32_t*>(W.A(W.sl.lbits)) +
+         (size_t)(level - 2) * (size_t)((W.sl.capC + 31) >> 5);
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// First candidate i in [start, end) with bound[i] > level-1 and ncnt[i] != 0
+// (src/IterFinderGpu.cu:26-34), or -1.  bits, when given, holds the
+// candidates with ncnt != 0.
+__device__ __forceinline__ int t1_next_live(const int32_t* bound, const int32_t* ncnt,
+                                            const uint32_t* bits, int start, int end, int level) {
+  const int lane = (int)lane_id();
+  if (!bits) {
+    for (int b0 = start; b0 < end; b0 += 32) {
+      const int i = b0 + lane;
+      const bool ok = i < end && bound[i] > level - 1 && ncnt[i] != 0;
+      const unsigned bal = __ballot_sync(kFull, ok);
+      if (bal) return b0 + __ffs(bal) - 1;
+    }
+    return -1;
+  }
+  if (start >= end) return -1;
+  const int w0 = start >> 5, wend = (end + 31) >> 5;
+  for (int wb = w0; wb < wend; wb += 32) {
+    const int w = wb + lane;
+    uint32_t m = w < wend ? bits[w] : 0u;
+    if (w == w0) m &= ~0u << (start & 31);
+    if (w == wend - 1 && (end & 31)) m &= (1u << (end & 31)) - 1u;
+    int first = -1;
+    while (m) {
+      const int i = (w << 5) + __ffs(m) - 1;
+      if (bound[i] > level - 1) {
+        first = i;
+        break;
+      }
+      m &= m - 1;
+    }
+    const unsigned bal = __ballot_sync(kFull, first >= 0);
+    if (bal) return __shfl_sync(kFull, first, __ffs(bal) - 1);
+  }
+  return -1;
+}
+
 __device__ void tier1_run(Warp& W, const T1& t) {
   const int lane = (int)lane_id();
   int32_t* llevel = W.A(W.sl.llevel);
   int32_t* ncnt = W.A(W.sl.ncnt);
   int32_t* bound = W.A(W.sl.bound);
   int32_t* stack = W.A(W.sl.stack);
-  int32_t* lsize = W.A(W.sl.lsize);
+  int32_t* lent = W.A(W.sl.lent);
   const uint64_t* ckey = W.A64(W.sl.ckey);
   const int32_t* coff = W.A(W.sl.coff);
   const int32_t* cadj = W.A(W.sl.cadj);
+  const int32_t* aoff = W.A(W.sl.aoff);
   const int32_t* aadj = W.A(W.sl.aadj);
   const bool emitting = W.p.emit != nullptr;
   const int t2max = W.gp->tier2_max_l;
+  const int cwords = (t.nC + 31) >> 5;
 
+  // The level bitmaps start clear (a task that ended early may leave bits).
+  for (int lv = 2; lv <= kLevelBits + 1; ++lv) {
+    uint32_t* b = level_bits(W, lv);
+    for (int w = lane; w < cwords; w += 32) b[w] = 0u;
+  }
   if (lane == 0) {
     stack[0] = t.nq;
-    lsize[0] = t.nL;
+    lent[0] = aoff[t.nL];
   }
   __syncwarp();
   int level = 1;
   while (level != 0) {
     if (must_stop(W)) return;
-    int cur = -1;
     const int end = level == 1 ? t.nend : t.nC;  // the first level may push a part only
-    for (int b0 = stack[level - 1]; b0 < end; b0 += 32) {
-      int i = b0 + lane;
-      bool ok = i < end && bound[i] > level - 1 && ncnt[i] != 0;
-      unsigned bal = __ballot_sync(kFull, ok);
-      if (bal) {
-        cur = b0 + __ffs(bal) - 1;
-        break;
-      }
-    }
+    int cur = t1_next_live(bound, ncnt, level_bits(W, level), stack[level - 1], end, level);
     if (cur >= 0) {
       // ---- finder_push (src/IterFinderGpu.h:206-264) ----
       W.pushes += 1;
       int kept = 0;
       uint64_t sL = 0;
+      long long kent = 0;                 // entries of the kept rows
+      unsigned long long best = ~0ULL;    // (row length << 32) | position of the shortest kept row
       int rb = coff[cur], re = coff[cur + 1];
       for (int j = rb + lane; j < re; j += 32) {
         int l = cadj[j];
@@ -1123,10 +1238,15 @@ __device__ void tier1_run(Warp& W, const T1& t) {
           llevel[l] = level;
           ++kept;
           sL += W.gp->ukey[t.L[l]];
+          const int len = aoff[l + 1] - aoff[l];
+          kent += len;
+          best = min(best, ((unsigned long long)(unsigned)len << 32) | (unsigned)l);
         }
       }
       kept = warp_sum(kept);
       sL = warp_sum(sL);
+      kent = warp_sum(kent);
+      best = warp_min_u64(best);
       __syncwarp();
       if (W.p.prune && kept <= t2max) {
         t1_sparse_push(W, t, cur, level, kept, sL);
@@ -1134,12 +1254,25 @@ __device__ void tier1_run(Warp& W, const T1& t) {
         __syncwarp();
         continue;
       }
-      int nLp = lsize[level - 1];
-      bool recompute = nLp > 2 * kept;
-      if (recompute) {
-        for (int i = lane; i < t.nC; i += 32) ncnt[i] = 0;
+      // Counts over the kept rows: subtract the removed rows, or clear the
+      // level's counts and add the kept rows, whichever walks less.
+      const uint32_t* pbits = level_bits(W, level);
+      const long long rent = (long long)lent[level - 1] - kent;
+      const long long clear_cost = pbits ? (long long)cwords : (long long)t.nC;
+      if (clear_cost + kent < rent) {
+        if (pbits) {
+          for (int w = lane; w < cwords; w += 32) {
+            uint32_t m = pbits[w];
+            while (m) {
+              ncnt[(w << 5) + __ffs(m) - 1] = 0;
+              m &= m - 1;
+            }
+          }
+        } else {
+          for (int i = lane; i < t.nC; i += 32) ncnt[i] = 0;
+        }
         __syncwarp();
-        t1_rows_at_level(W, t, level, [&](bool valid, int, int pos) {
+        t1_rows_of(W, cur, level, [&](bool valid, int, int pos) {
           if (!valid) return;
           int p = aadj[pos];
           if (p >= 0) atomicAdd(&ncnt[p], 1);
@@ -1152,16 +1285,24 @@ __device__ void tier1_run(Warp& W, const T1& t) {
         });
       }
       __syncwarp();
+      // Maximality (src/IterFinderGpu.h:252-261): a candidate covering the new
+      // L is adjacent to every kept row, the shortest one included, so only
+      // that row's candidates are examined.
       bool ism = true;
       uint64_t sR = 0;
       unsigned long long nR = 0;
-      for (int i = lane; i < t.nC; i += 32) {
-        if (ncnt[i] == kept) {
-          sR += ckey[i];
-          ++nR;
-          int b = bound[i];
-          if (i < cur && b >= level) ism = false;
-          else if (b > level) bound[i] = level;
+      {
+        const int lstar = (int)(best & 0xffffffffu);
+        const int mb = aoff[lstar], me = aoff[lstar + 1];
+        for (int j = mb + lane; j < me; j += 32) {
+          const int i = aadj[j];
+          if (i >= 0 && ncnt[i] == kept) {
+            sR += ckey[i];
+            ++nR;
+            int b = bound[i];
+            if (i < cur && b >= level) ism = false;
+            else if (b > level) bound[i] = level;
+          }
         }
       }
       ism = __all_sync(kFull, ism);
@@ -1183,7 +1324,15 @@ __device__ void tier1_run(Warp& W, const T1& t) {
           if (lane == 0) {
             stack[level - 1] = cur;
             stack[level] = cur + 1;
-            lsize[level] = kept;
+            lent[level] = (int32_t)kent;
+          }
+          uint32_t* nbits = level_bits(W, level + 1);
+          if (nbits) {
+            t1_rows_of(W, cur, level, [&](bool valid, int, int pos) {
+              if (!valid) return;
+              const int p = aadj[pos];
+              if (p >= 0) atomicOr(&nbits[p >> 5], 1u << (p & 31));
+            });
           }
           __syncwarp();
           ++level;
@@ -1198,6 +1347,15 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       if (level > 0) {
         cur = stack[level - 1];
         __syncwarp();
+        uint32_t* cbits = level_bits(W, level + 1);
+        if (cbits) {  // the finished level's bitmap back to clear
+          t1_rows_of(W, cur, level, [&](bool valid, int, int pos) {
+            if (!valid) return;
+            const int p = aadj[pos];
+            if (p >= 0) cbits[p >> 5] = 0u;
+          });
+          __syncwarp();
+        }
         t1_pop(W, t, cur, level);
         if (lane == 0) stack[level - 1] = cur + 1;
         __syncwarp();

@@ -10,6 +10,7 @@ namespace gmbe {
 constexpr int kEnumWarps = 16;                 // warps per block
 constexpr int kEnumThreads = kEnumWarps * 32;  // threads per block
 constexpr int kKMax = 4;                       // bitmap words of the tier-2 sub-problem
+constexpr int kLevelBits = 8;                  // counts-tier levels with a candidate bitmap
 
 // One persistent launch over p.n_graphs graphs: graphs[i] describes graph i,
 // root_prefix[i] counts the roots of graphs before i (root_prefix[n] = all),

@@ -13,7 +13,8 @@
 // independent, so a sample of roots is a sample of its work.  Sample j
 // (j = first .. first+count-1) is the roots v = j, j + stride, j + 2 stride,
 // ... below max_root (positions in the reference's own internal order after
-// -t/-o, from the lowest degree up).  The roots of a sample run on `threads`
+// -t/-o, from the lowest degree up; a max_root below 1 is that fraction of
+// all roots, 0 = every root).  The roots of a sample run on `threads`
 // OpenMP threads, one finder object per thread (the finder's only mutable
 // state is its counter).  One line per sample:
 //   sample <j> roots <n> count <bicliques> seconds <wall time of the sample>
@@ -40,8 +41,11 @@
 #undef protected
 
 static int run_samples(CSRBiGraph* graph, int stride, int first, int count, int threads,
-                       int max_root) {
+                       double max_root_arg) {
   if (stride < 1 || first < 0 || count < 1 || threads < 1) return 2;
+  long long max_root = max_root_arg > 0 && max_root_arg < 1
+                           ? (long long)(max_root_arg * graph->V_size)
+                           : (long long)max_root_arg;
   if (max_root <= 0 || max_root > graph->V_size) max_root = graph->V_size;
   std::vector<MbeaFinderBitset*> finders;
   for (int t = 0; t < threads; ++t) finders.push_back(new MbeaFinderBitset(graph));
@@ -92,7 +96,7 @@ int main(int argc, char** argv) {
            graph->U_size, graph->edge_size);
     fflush(stdout);
     rc = run_samples(graph, atoi(argv[5]), atoi(argv[6]), atoi(argv[7]), atoi(argv[8]),
-                     atoi(argv[9]));
+                     atof(argv[9]));
   } else {
     BicliqueFinder* finder = nullptr;
     if (sel == 0)

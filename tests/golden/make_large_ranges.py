@@ -79,7 +79,7 @@ def main():
         dt = time.perf_counter() - t
         ranges.append({"root_begin": a, "root_end": b, "count": int(o.count),
                        "set_hash": f"{o.set_hash:#018x}", "max_two_hop": int(s_int[a:b].max()),
-                       "oracle_seconds": round(dt, 1)})
+                       "alg_bytes": int(o.alg_bytes), "oracle_seconds": round(dt, 1)})
         print(ranges[-1], flush=True)
     with open(OUT, "w") as f:
         json.dump({"generator": "tests/golden/make_large_ranges.py", "config": "large",

@@ -47,7 +47,7 @@ def main():
         dt = time.perf_counter() - t
         shards.append({"shard_index": off, "shard_count": STRIDE, "count": int(o.count),
                        "set_hash": f"{o.set_hash:#018x}", "non_maximal": int(o.non_maximal),
-                       "oracle_seconds": round(dt, 1)})
+                       "alg_bytes": int(o.alg_bytes), "oracle_seconds": round(dt, 1)})
         print(shards[-1], flush=True)
         with open(OUT, "w") as f:
             json.dump({"generator": "tests/golden/make_large_shards.py", "config": "large",

@@ -343,6 +343,24 @@ def test_sharded_ranks_sum_to_the_whole_graph():
     assert 0 < half.count < want.count
 
 
+def test_batch_oracle_fixture_reproduces(gm):
+    # tests/golden/batch_oracle.json (all 4,096 batched graphs) agrees with
+    # the reference-pinned golden cases for seeds 1000..1002 and with the
+    # oracle rerun on a spread of its graphs.
+    with open(os.path.join(ROOT, "tests", "golden", "batch_oracle.json")) as f:
+        d = json.load(f)
+    assert d["n"] == len(d["count"]) == len(d["set_hash"]) == 4096
+    assert sum(d["count"]) == d["total_count"]
+    gold = _golden_cases()
+    for i in range(3):
+        c = gold[f"batch_{1000 + i}"]
+        assert (d["count"][i], d["set_hash"][i]) == (c["oracle_count"], c["oracle_set_hash"])
+    for i in (5, 777, 2048, 4095):
+        g = gm.batch_graph(d["first_seed"] + i)
+        o = oracle.gmbe(g.row_off, g.col, g.nU, uvtrans=1, order=1)
+        assert (o.count, f"{o.set_hash:#018x}") == (d["count"][i], d["set_hash"][i])
+
+
 @pytest.fixture(scope="module")
 def large_graph(gm):
     return gm.config_graph("large")

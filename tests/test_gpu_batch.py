@@ -74,3 +74,24 @@ def test_batch_split_modes(gm, split_mode):
         per, _ = B.run(split_mode=split_mode)
     for r, w in zip(per, want):
         assert (r.count, r.set_hash) == (w.count, w.set_hash)
+
+
+@pytest.mark.last
+def test_full_batched_workload_matches_oracle_fixture(gm):
+    # The whole batched workload (4,096 graphs, seeds 1000..5095) in one
+    # launch: every per-graph count and set hash on two replays equals the
+    # CPU oracle's, committed in tests/golden/batch_oracle.json
+    # (tests/golden/make_batch_oracle.py).
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "batch_oracle.json")
+    with open(path) as f:
+        orc = json.load(f)
+    want = list(zip(orc["count"], (int(h, 16) for h in orc["set_hash"])))
+    gs = [gm.batch_graph(orc["first_seed"] + i) for i in range(orc["n"])]
+    with gm.Batch(gs) as B:
+        for rep in range(2):
+            per, tot = B.run()
+            bad = [i for i, r in enumerate(per) if (r.count, r.set_hash) != want[i]]
+            assert not bad, (rep, bad[:10])
+            assert tot.count == orc["total_count"]

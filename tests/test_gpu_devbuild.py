@@ -1,11 +1,12 @@
 """Graph build on the device (mbe_graph_build_on_device) against the host build
 and the oracle.
 
-The device build orders rows of equal degree by input position rather than
-lexicographically, so internal ids may differ from the host build's; the
-enumerated set may not.  The bar is bit-exact equality of count and set hash
-with the oracle and the golden fixtures, equal graph summaries, equal emitted
-sets, and the host build's error codes on malformed input.
+The device build orders rows exactly as the host build does (size, then
+content, then original id), so both have the same internal ids: root shards
+and ranges enumerate the same roots.  The bar is bit-exact equality of count
+and set hash with the oracle and the golden fixtures, per shard with the host
+build, equal graph summaries, equal emitted sets, and the host build's error
+codes on malformed input.
 """
 import numpy as np
 import pytest
@@ -50,23 +51,35 @@ def test_summary_and_result_equal_host_build(gm, uvtrans, order):
                 gm.Graph.build_on_device(ro, co, nU, **opts) as D:
             assert info_tuple(D) == info_tuple(H)
             rh, rd = H.enumerate(), D.enumerate()
-        assert (rd.count, rd.set_hash) == (rh.count, rh.set_hash)
+            assert (rd.count, rd.set_hash) == (rh.count, rh.set_hash)
+            # same internal order: every shard holds the same roots
+            for si in range(5):
+                a = H.enumerate(shard_count=5, shard_index=si)
+                b = D.enumerate(shard_count=5, shard_index=si)
+                assert (b.count, b.set_hash) == (a.count, a.set_hash), si
 
 
-def test_equal_degrees_keep_input_order(gm):
-    # Every row of degree 3: the degree sort is a no-op for the device build
-    # and a lexicographic reordering for the host build.
+def test_equal_degrees_follow_the_host_order(gm):
+    # Every row of degree 3 (identical rows included): the order is decided
+    # by row content and original id alone, as in the host build.
     rng = np.random.default_rng(4)
     nV, nU = 120, 40
     rows = [np.sort(rng.choice(nU, 3, replace=False)).astype(np.int32) for _ in range(nV)]
+    rows[7] = rows[3]
+    rows[50] = rows[3]
     ro = np.zeros(nV + 1, np.int32)
     ro[1:] = np.cumsum([3] * nV)
     co = np.concatenate(rows)
     want = oracle.gmbe(ro, co, nU)
     for order in (0, 1, 2):
-        with gm.Graph.build_on_device(ro, co, nU, uvtrans=0, order=order) as D:
+        with gm.Graph.from_csr(ro, co, nU, uvtrans=0, order=order) as H, \
+                gm.Graph.build_on_device(ro, co, nU, uvtrans=0, order=order) as D:
             r = D.enumerate()
-        assert (r.count, r.set_hash) == (want.count, want.set_hash)
+            assert (r.count, r.set_hash) == (want.count, want.set_hash)
+            for si in range(7):
+                a = H.enumerate(shard_count=7, shard_index=si)
+                b = D.enumerate(shard_count=7, shard_index=si)
+                assert (b.count, b.set_hash) == (a.count, a.set_hash), (order, si)
 
 
 def test_wide_id_range(gm):
