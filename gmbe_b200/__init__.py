@@ -61,8 +61,9 @@ class Params(C.Structure):
                 ("root_split_size", C.c_int32), ("share_min_work", C.c_int32),
                 ("range_split_work", C.c_int32), ("range_chunk", C.c_int32),
                 ("eager_share", C.c_int32), ("big_two_hop", C.c_int32),
-                ("big_warps", C.c_int32), ("reserved_p", C.c_int32),
-                ("time_limit_ns", C.c_int64)]
+                ("big_warps", C.c_int32), ("l2_window", C.c_int32),
+                ("time_limit_ns", C.c_int64), ("touch_scan", C.c_int32),
+                ("reserved_q", C.c_int32)]
 
 
 class Result(C.Structure):

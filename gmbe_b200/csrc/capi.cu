@@ -140,6 +140,9 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
   };
   const int64_t C = capC, Lc = capL, S = capS, T2 = 32 * kKMax;
   s.map = take(nV);
+  s.gseen_words = (int32_t)((std::max<int64_t>(nV, C) + 31) / 32);
+  s.gseen = take(s.gseen_words);
+  s.zero_words = off;
   s.touched = take(C);
   s.cv = take(C);
   s.ncnt = take(C);
@@ -368,6 +371,7 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.slot_spin_limit = 20000000;  // x ~64 ns sleeps: a claimed slot is written within microseconds
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
   ep.time_limit_ns = std::max<int64_t>(prm.time_limit_ns, 0);
+  ep.touch_scan = prm.touch_scan > 0 ? 1 : (prm.touch_scan < 0 ? -1 : 0);
   ep.record_exit = prm.sm_timing ? 1 : 0;
   ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
   // Heavy roots split into vertex tuples (sub-problem sharing mode only).
@@ -378,9 +382,10 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.n_graphs = spec.n_graphs;
   ep.n_big_warps = n_big;
   ep.big_sl = big_sl;
-  if (n_big > 0) {  // vertex-tuple children and root parts could need the big tier
+  if (n_big > 0) {
+    // Vertex-tuple children could need the big tier: off.  Root parts stay
+    // available (a big root's parts go to big warps only).
     ep.root_split = 0;
-    ep.range_work = 0;
   }
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;
@@ -390,15 +395,17 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
 
 int engine_clear_maps(Workspace& ws, LaunchPlan* plan, cudaStream_t st) {
   if (!plan->clear_maps) return MBE_OK;
-  // The count map is the first slice of either layout.
-  const size_t width = (size_t)std::max<int32_t>(plan->map_words, 1) * sizeof(int32_t);
+  // The count map and the global first-touch bitmap are the first slices of
+  // either layout.
   const int n_big = plan->ep.n_big_warps;
   const size_t big_pitch = (size_t)plan->ep.big_sl.words_per_warp;
   if (n_big > 0)
-    CK(cudaMemset2DAsync(ws.scratch, big_pitch * sizeof(int32_t), 0, width, (size_t)n_big, st));
+    CK(cudaMemset2DAsync(ws.scratch, big_pitch * sizeof(int32_t), 0,
+                         (size_t)plan->ep.big_sl.zero_words * sizeof(int32_t), (size_t)n_big, st));
   if (plan->warps > n_big)
     CK(cudaMemset2DAsync(ws.scratch + big_pitch * (size_t)n_big,
-                         (size_t)plan->sl.words_per_warp * sizeof(int32_t), 0, width,
+                         (size_t)plan->sl.words_per_warp * sizeof(int32_t), 0,
+                         (size_t)plan->sl.zero_words * sizeof(int32_t),
                          (size_t)(plan->warps - n_big), st));
   ws.map_pitch_words = plan->sl.words_per_warp;
   ws.map_words = plan->map_words;
@@ -420,10 +427,26 @@ int engine_enqueue(Workspace& ws, LaunchPlan* plan, const DevGraph* d_graphs,
   CK(cudaMemsetAsync(d_gres, 0, 3 * sizeof(unsigned long long) * (size_t)n_graphs, st));
   if (ev0) CK(cudaEventRecord(ev0, st));
   auto* kernel = plan->ep.n_big_warps > 0 ? mbe_enum_kernel_tiers : mbe_enum_kernel;
-  kernel<<<plan->blocks, kEnumThreads, enum_smem_bytes(plan->sl), st>>>(
-      d_graphs, d_prefix, d_gres, plan->ep, plan->sl, ws.ctl, ws.q_tasks, ws.q_seq, plan->pool,
-      ws.scratch, ws.exit_ns);
-  CK(cudaGetLastError());
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)plan->blocks);
+  cfg.blockDim = dim3(kEnumThreads);
+  cfg.dynamicSmemBytes = enum_smem_bytes(plan->sl);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  if (plan->l2_bytes > 0) {
+    // The hot read-only data (the graph's U -> V lists, walked by every task
+    // set-up) persists in L2 while the warps' scratch streams through it.
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(plan->l2_base);
+    attr[0].val.accessPolicyWindow.num_bytes = plan->l2_bytes;
+    attr[0].val.accessPolicyWindow.hitRatio = plan->l2_hit;
+    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  CK(cudaLaunchKernelEx(&cfg, kernel, d_graphs, d_prefix, d_gres, plan->ep, plan->sl, ws.ctl,
+                        ws.q_tasks, ws.q_seq, plan->pool, ws.scratch, ws.exit_ns));
   if (ev1) CK(cudaEventRecord(ev1, st));
   return MBE_OK;
 }
@@ -708,12 +731,41 @@ static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* o
       CK(cudaMalloc((void**)&ws.big_flag, big_flags.size()));
       ws.big_flag_cap = big_flags.size();
     }
+    if (big_list.size() > ws.big_parts_cap) {
+      cudaFree(ws.big_parts);
+      ws.big_parts = nullptr;
+      ws.big_parts_cap = 0;
+      CK(cudaMalloc((void**)&ws.big_parts, 4 * sizeof(int32_t) * big_list.size()));
+      ws.big_parts_cap = big_list.size();
+    }
     CK(cudaMemcpyAsync(ws.big_roots, big_list.data(), sizeof(int32_t) * big_list.size(),
                        cudaMemcpyHostToDevice, 0));
     CK(cudaMemcpyAsync(ws.big_flag, big_flags.data(), big_flags.size(), cudaMemcpyHostToDevice, 0));
+    CK(cudaMemsetAsync(ws.big_parts, 0, 4 * sizeof(int32_t) * big_list.size(), 0));
     plan.ep.n_big_roots = (int32_t)big_list.size();
     plan.ep.big_roots = ws.big_roots;
     plan.ep.big_flag = ws.big_flag;
+    plan.ep.big_parts = ws.big_parts;
+    plan.ep.big_parts_cap = (int32_t)big_list.size();
+  }
+  if (prm.l2_window >= 0) {
+    // The persisting L2 limit is a setting of this process's context (the
+    // device's own configuration is untouched); set once per device.
+    if (ws.l2_persist < 0) {
+      int persist = 0, maxw = 0;
+      CK(cudaDeviceGetAttribute(&persist, cudaDevAttrMaxPersistingL2CacheSize, g->device));
+      CK(cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, g->device));
+      ws.l2_persist = persist > 0 && maxw > 0 ? persist : 0;
+      ws.l2_max_window = maxw;
+      if (ws.l2_persist > 0) CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)persist));
+    }
+    const size_t bytes = std::min<size_t>(sizeof(int32_t) * (size_t)h.edge_size,
+                                          (size_t)ws.l2_max_window);
+    if (ws.l2_persist > 0 && bytes > 0) {
+      plan.l2_base = g->d_rev_col;
+      plan.l2_bytes = bytes;
+      plan.l2_hit = (float)std::min(1.0, (double)ws.l2_persist / (double)bytes);
+    }
   }
   long long prefix[2] = {0, n_roots};
   CK(cudaMemcpyAsync(ws.d_graph1, &dg, sizeof(dg), cudaMemcpyHostToDevice, 0));
@@ -724,6 +776,7 @@ static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* o
   unsigned long long gres[3];
   CK(cudaMemcpy(&ctl, ws.ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(gres, ws.d_gres1, sizeof(gres), cudaMemcpyDeviceToHost));
+  if (plan.l2_bytes > 0) CK(cudaCtxResetPersistingL2Cache());  // later work gets the L2 back
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, ws.ev0, ws.ev1));
   out->count = gres[0];

@@ -42,6 +42,11 @@ struct Workspace {
   int32_t* big_roots = nullptr;
   uint8_t* big_flag = nullptr;
   size_t big_roots_cap = 0, big_flag_cap = 0;
+  int32_t* big_parts = nullptr;  // part records of big roots (4 int32 each)
+  size_t big_parts_cap = 0;
+  // Persisting L2 of the device (bytes; -1 = not queried yet, 0 = none).
+  long long l2_persist = -1;
+  int l2_max_window = 0;
   // Bumped whenever a buffer above is (re)allocated: a captured launch that
   // refers to an older generation must be captured again.
   uint64_t gen = 1;
@@ -98,6 +103,10 @@ struct LaunchPlan {
   SlotPool pool;
   bool clear_maps = false;
   int32_t map_words = 1;
+  // Persisting L2 access-policy window of the launch (l2_bytes 0: none).
+  const void* l2_base = nullptr;
+  size_t l2_bytes = 0;
+  float l2_hit = 1.0f;
 };
 
 // Device bytes of the scratch of `warps` warps, n_big of them with the big

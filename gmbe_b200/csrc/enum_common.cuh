@@ -73,6 +73,8 @@ struct EnumCtl {
   unsigned long long n_tasks, n_tier2;
   unsigned long long emit_pos;  // words of biclique records reserved (may pass the buffer's end)
   long long next_big;           // entries of the big-root list handed out so far
+  unsigned long long n_big_parts;     // part records appended (may pass big_parts_cap)
+  unsigned long long big_parts_head;  // first part record that may have unclaimed parts
 };
 
 // Per-warp scratch layout (int32 words unless noted), offsets in words from
@@ -95,6 +97,14 @@ struct ScratchLayout {
   // Words per warp of the first-touch bitmap in shared memory (one bit per
   // V vertex / candidate position); 0 = first touches found by global atomics.
   int32_t seen_words;
+  // A first-touch bitmap in global memory (one bit per V vertex / candidate
+  // position, gseen_words words), right after the count map: large counting
+  // passes without the shared one mark touches with fire-and-forget atomics
+  // and collect them by a scan of its words.  Words [0, zero_words) of every
+  // warp (count map and this bitmap) are all-zero between tasks.
+  int64_t gseen;
+  int32_t gseen_words;
+  int64_t zero_words;
 };
 
 // Slots for bitmap sub-problems handed to idle warps.
@@ -149,6 +159,8 @@ struct EnumParams {
   int64_t slot_spin_limit;    // iterations waiting for a claimed slot to be written
   int64_t idle_ns_limit;      // nanoseconds a warp may idle waiting for work
   int64_t time_limit_ns;      // > 0: the launch gives up after this long (kStDeadline)
+  int32_t touch_scan;         // 0 auto, 1 always scan the global touch bitmap, -1 never
+  int32_t pad_ts;
   int32_t record_exit;        // -p
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)
@@ -171,6 +183,10 @@ struct EnumParams {
   const int32_t* big_roots;
   const uint8_t* big_flag;
   ScratchLayout big_sl;
+  // Parts of listed big roots (only big warps may run them): records of four
+  // int32 {root, parts, next part to claim, ready}, all-zero at launch.
+  int32_t* big_parts;
+  int32_t big_parts_cap;
 };
 
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {

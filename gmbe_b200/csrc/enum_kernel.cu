@@ -113,6 +113,7 @@ struct Warp {
   unsigned long long ns_t1;        // time inside the counts tier (bitmap tier excluded)
   uint32_t* seen;                  // this warp's first-touch bitmap in shared memory, or null
   uint64_t deadline;               // %globaltimer after which the launch gives up (0: never)
+  uint32_t* gseen;                 // this warp's first-touch bitmap in global memory
 
   __device__ int32_t* A(int64_t off) const { return base + off; }
   __device__ uint64_t* A64(int64_t off) const { return reinterpret_cast<uint64_t*>(base + off); }
@@ -141,6 +142,41 @@ __device__ __forceinline__ void counts_done(const Warp& W, const int32_t* idx, i
     for (int i = (int)lane_id(); i < n; i += 32) W.seen[idx[i] >> 5] = 0u;
     __syncwarp();
   }
+}
+
+// Whether a counting pass of `entries` entries over an index space of
+// `words` bitmap words collects its first touches from the global bitmap:
+// only without the shared-memory bitmap, and when the pass is large enough
+// that a scan of the words costs less than an atomic round trip per 32
+// entries.
+__device__ __forceinline__ bool use_gseen(const Warp& W, long long entries, int words) {
+  if (W.p.touch_scan != 0) return W.p.touch_scan > 0;
+  return W.seen == nullptr && entries >= (long long)words;
+}
+
+// Lists the set bits of bits[0, words) in increasing index order into
+// out[0, cap) (indices beyond cap are not written) and clears the words;
+// returns the number of set bits.  Every lane takes one word per round, so
+// the loads are independent and coalesced.  The bits were set by this warp's
+// atomics: the fence before the call makes them visible here.
+__device__ int collect_bits(uint32_t* bits, int words, int32_t* out, int cap) {
+  const int lane = (int)lane_id();
+  int n = 0;
+  for (int w0 = 0; w0 < words; w0 += 32) {
+    const int w = w0 + lane;
+    uint32_t m = w < words ? __ldcg(bits + w) : 0u;
+    if (m) bits[w] = 0u;
+    int tot;
+    int o = n + warp_excl_scan(__popc(m), &tot);
+    while (m) {
+      if (o < cap) out[o] = (w << 5) + __ffs(m) - 1;
+      ++o;
+      m &= m - 1;
+    }
+    n += tot;
+  }
+  __syncwarp();
+  return n;
 }
 
 // Emission (opt-in): appends a maximal biclique's L to the launch's record
@@ -1009,26 +1045,54 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   int32_t* tcls = W.A(W.sl.tcls);
   const uint64_t* ckey = W.A64(W.sl.ckey);
   int nt = 0, ne = 0;
-  flat_rows(
-      n,
-      [&](int r, int& beg, int& len) {
-        int l = lp[r];
-        beg = aoff[l];
-        len = aoff[l + 1] - beg;
-      },
-      [&](bool valid, int r, int pos) {
-        int p = valid ? aadj[pos] : -1;
-        bool first = false;
-        if (p >= 0) first = count_first(W, cc, p);
-        const unsigned lt = lanemask_lt();
-        unsigned bal = __ballot_sync(kFull, first);
-        if (first) tl[nt + __popc(bal & lt)] = p;
-        nt += __popc(bal);
-        unsigned be = __ballot_sync(kFull, p >= 0);
-        if (p >= 0) ent[ne + __popc(be & lt)] = (p << 7) | r;
-        ne += __popc(be);
-      });
-  counts_done(W, tl, nt);
+  int kent = 0;  // entries of the kept rows
+  for (int q = lane; q < n; q += 32) kent += aoff[lp[q] + 1] - aoff[lp[q]];
+  kent = warp_sum(kent);
+  const int cwords = (t.nC + 31) >> 5;
+  if (use_gseen(W, kent, cwords)) {
+    // fire-and-forget counts and touch bits; the touched list from the bitmap
+    flat_rows(
+        n,
+        [&](int r, int& beg, int& len) {
+          int l = lp[r];
+          beg = aoff[l];
+          len = aoff[l + 1] - beg;
+        },
+        [&](bool valid, int r, int pos) {
+          int p = valid ? aadj[pos] : -1;
+          if (p >= 0) {
+            atomicAdd(&cc[p], 1);
+            atomicOr(&W.gseen[p >> 5], 1u << (p & 31));
+          }
+          const unsigned be = __ballot_sync(kFull, p >= 0);
+          if (p >= 0) ent[ne + __popc(be & lanemask_lt())] = (p << 7) | r;
+          ne += __popc(be);
+        });
+    __threadfence_block();
+    __syncwarp();
+    nt = collect_bits(W.gseen, cwords, tl, t.nC);
+  } else {
+    flat_rows(
+        n,
+        [&](int r, int& beg, int& len) {
+          int l = lp[r];
+          beg = aoff[l];
+          len = aoff[l + 1] - beg;
+        },
+        [&](bool valid, int r, int pos) {
+          int p = valid ? aadj[pos] : -1;
+          bool first = false;
+          if (p >= 0) first = count_first(W, cc, p);
+          const unsigned lt = lanemask_lt();
+          unsigned bal = __ballot_sync(kFull, first);
+          if (first) tl[nt + __popc(bal & lt)] = p;
+          nt += __popc(bal);
+          unsigned be = __ballot_sync(kFull, p >= 0);
+          if (p >= 0) ent[ne + __popc(be & lt)] = (p << 7) | r;
+          ne += __popc(be);
+        });
+    counts_done(W, tl, nt);
+  }
   // R of the child, maximality, and each touched candidate's class (0 none,
   // 1 Q, 2 P).  Lane-local counters keep the iterations independent, so
   // their loads overlap.
@@ -1480,6 +1544,55 @@ __device__ bool queue_push_parts(Warp& W, const Task& t, int m) {
   });
 }
 
+// Parts 1 .. m-1 of a listed big root (lane-uniform): a part record that only
+// big warps claim from (the other warps' scratch cannot hold the root).
+// They count as pending before the record becomes visible.  False if the
+// record list is full (the root then runs whole).
+__device__ bool big_parts_push(Warp& W, int v, int m) {
+  int ok = 0;
+  if (lane_id() == 0) {
+    const unsigned long long i = atomicAdd(&W.ctl->n_big_parts, 1ULL);
+    if (i < (unsigned long long)W.p.big_parts_cap) {
+      atomicAdd(&W.ctl->pending, (unsigned long long)(m - 1));
+      int32_t* r = W.p.big_parts + 4 * i;
+      r[0] = v;
+      r[1] = m;
+      r[2] = 1;  // part 0 runs on this warp
+      __threadfence();
+      atomicExch(&r[3], 1);
+      ok = 1;
+    }
+  }
+  return __shfl_sync(kFull, ok, 0) != 0;
+}
+
+// Claims a part of a listed big root (lane 0 of a big warp).
+__device__ bool big_parts_claim(Warp& W, Task* t) {
+  EnumCtl* c = W.ctl;
+  const unsigned long long n = min(*(volatile unsigned long long*)&c->n_big_parts,
+                                   (unsigned long long)W.p.big_parts_cap);
+  for (unsigned long long i = *(volatile unsigned long long*)&c->big_parts_head; i < n; ++i) {
+    int32_t* r = W.p.big_parts + 4 * i;
+    if (*(volatile int32_t*)&r[3] == 0) continue;  // being written
+    const int m = *(volatile int32_t*)&r[1];
+    if (*(volatile int32_t*)&r[2] < m) {
+      const int j = atomicAdd(&r[2], 1);
+      if (j < m) {
+        t->v[0] = *(volatile int32_t*)&r[0];
+        t->v[1] = t->v[2] = t->v[3] = -1;
+        t->graph = 0;
+        t->part = j;
+        t->parts = m;
+        t->pad = 0;
+        return true;
+      }
+    }
+    // exhausted: move the head past it (another warp may have done so)
+    atomicCAS(&c->big_parts_head, i, i + 1);
+  }
+  return false;
+}
+
 // Pushes one task (lane-uniform); false if the ring is full.
 __device__ bool queue_push_one(Warp& W, const Task& t) {
   const int lane = (int)lane_id();
@@ -1595,24 +1708,50 @@ __device__ void run_task(Warp& W, const Task& t) {
   }
   __syncwarp();
   int nt = 0;
-  flat_rows(
-      nL,
-      [&](int r, int& beg, int& len) {
-        int u = L[r];
-        beg = g.rev_off[u];
-        len = g.rev_off[u + 1] - beg;
-      },
-      [&](bool valid, int, int pos) {
-        int w = valid ? __ldg(g.rev_col + pos) : 0;
-        bool isnew = valid && count_first(W, map, w);
-        unsigned bal = __ballot_sync(kFull, isnew);
-        if (isnew) touched[nt + __popc(bal & lanemask_lt())] = w;
-        nt += __popc(bal);
-      });
-  counts_done(W, touched, min(nt, W.sl.capC));
+  const int vwords = (g.nV + 31) >> 5;
+  if (use_gseen(W, aoff[nL], vwords)) {
+    // Large set-up without the shared bitmap: fire-and-forget counts and
+    // touch bits, then the touched list in id order from the bitmap.
+    flat_rows(
+        nL,
+        [&](int r, int& beg, int& len) {
+          int u = L[r];
+          beg = g.rev_off[u];
+          len = g.rev_off[u + 1] - beg;
+        },
+        [&](bool valid, int, int pos) {
+          if (!valid) return;
+          const int w = __ldg(g.rev_col + pos);
+          atomicAdd(&map[w], 1);
+          atomicOr(&W.gseen[w >> 5], 1u << (w & 31));
+        });
+    __threadfence_block();
+    __syncwarp();
+    nt = collect_bits(W.gseen, vwords, touched, W.sl.capC);
+  } else {
+    flat_rows(
+        nL,
+        [&](int r, int& beg, int& len) {
+          int u = L[r];
+          beg = g.rev_off[u];
+          len = g.rev_off[u + 1] - beg;
+        },
+        [&](bool valid, int, int pos) {
+          int w = valid ? __ldg(g.rev_col + pos) : 0;
+          bool isnew = valid && count_first(W, map, w);
+          unsigned bal = __ballot_sync(kFull, isnew);
+          if (isnew && nt + __popc(bal & lanemask_lt()) < W.sl.capC)
+            touched[nt + __popc(bal & lanemask_lt())] = w;
+          nt += __popc(bal);
+        });
+    counts_done(W, touched, min(nt, W.sl.capC));
+  }
   if (nt > W.sl.capC) {
+    // Vertices beyond the touched list's room keep counts: clear the whole
+    // map (the launch is failing; this keeps the invariant for the record).
     set_status(W.ctl, kStCapacity, ((unsigned long long)3 << 32) | (unsigned)nt);
-    for (int i = lane; i < nt && i < W.sl.capC; i += 32) map[touched[i]] = 0;
+    for (int i = lane; i < g.nV; i += 32) map[i] = 0;
+    __syncwarp();
     return;
   }
 
@@ -1652,7 +1791,10 @@ __device__ void run_task(Warp& W, const Task& t) {
         np_all >= 2 * W.p.range_chunk &&
         (long long)np_all * cntC > (long long)W.p.range_work) {
       const int m = min((np_all + W.p.range_chunk - 1) / W.p.range_chunk, kMaxParts);
-      if (queue_push_parts(W, t, m)) {
+      // A listed big root's parts go to big warps only; other roots' parts
+      // fit every warp and take the common queue.
+      const bool big_root = W.p.n_big_warps > 0 && W.p.big_flag[last];
+      if (big_root ? big_parts_push(W, last, m) : queue_push_parts(W, t, m)) {
         part = 0;
         parts = m;
         W.splits += 1;
@@ -2030,7 +2172,10 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
                  : scratch + (size_t)p.n_big_warps * (size_t)p.big_sl.words_per_warp +
                        (size_t)(warp_global - p.n_big_warps) * (size_t)sl.words_per_warp;
   extern __shared__ uint32_t enum_smem[];
-  W.seen = sl.seen_words ? enum_smem + (size_t)(threadIdx.x >> 5) * sl.seen_words : nullptr;
+  W.seen = sl.seen_words && p.touch_scan <= 0
+               ? enum_smem + (size_t)(threadIdx.x >> 5) * sl.seen_words
+               : nullptr;
+  W.gseen = reinterpret_cast<uint32_t*>(W.base + W.sl.gseen);
   if (W.seen) {
     for (int i = lane; i < sl.seen_words; i += 32) W.seen[i] = 0u;
     __syncwarp();
@@ -2059,8 +2204,11 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
       if (!have && p.server) {
         have = serve_claim_root(W, &t) ? 1 : 0;
       } else if (!have) {
-        // A big warp first takes the roots no other warp has room for.
-        if (kTiers && big && *(volatile long long*)&ctl->next_big < (long long)p.n_big_roots) {
+        // A big warp first takes parts of big roots, then the roots no other
+        // warp has room for.
+        if (kTiers && big && p.big_parts_cap > 0) have = big_parts_claim(W, &t) ? 1 : 0;
+        if (!have && kTiers && big &&
+            *(volatile long long*)&ctl->next_big < (long long)p.n_big_roots) {
           atomicAdd(&ctl->pending, 1ULL);
           long long b = (long long)atomicAdd((unsigned long long*)&ctl->next_big, 1ULL);
           if (b < (long long)p.n_big_roots) {

@@ -48,6 +48,7 @@ constexpr int32_t kServeShareMinWorkDefault = 64;
 // P candidates per part of a root split into parts.
 constexpr int32_t kRangeChunkDefault = 64;
 
+
 // Per-warp scratch layout for the given capacities.
 ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS);
 

@@ -178,12 +178,13 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   int32_t* scratch = reinterpret_cast<int32_t*>(pool + o_scr);
 
   // The pool keeps the previous call's contents: zero what must start at
-  // zero (control block, ring slot tags, every warp's dense count map).
+  // zero (control block, ring slot tags, every warp's dense count map and
+  // first-touch bitmap).
   if ((e = cudaMemsetAsync(ctl, 0, sizeof(EnumCtl), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(q_seq, 0, sizeof(unsigned long long) * kNoAllocQueueCap, st)) !=
           cudaSuccess ||
       (e = cudaMemset2DAsync(scratch, (size_t)sl.words_per_warp * sizeof(int32_t), 0,
-                             (size_t)std::max(nV, 1) * sizeof(int32_t), (size_t)warps, st)) !=
+                             (size_t)sl.zero_words * sizeof(int32_t), (size_t)warps, st)) !=
           cudaSuccess)
     return set_error(MBE_ERR_CUDA, "clearing the pool: %s", cudaGetErrorString(e));
   noalloc_keys<<<std::max(1, std::min(1024, (nU + nV + 255) / 256)), 256, 0, st>>>(ukey, nU, vkey,

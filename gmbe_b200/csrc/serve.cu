@@ -156,7 +156,7 @@ int allocate(mbe_server* s) {
   SCK(cudaMalloc((void**)&s->d_scratch, scratch));
   // Every warp's count map starts all-zero; each task leaves it so.
   SCK(cudaMemset2D(s->d_scratch, (size_t)s->sl.words_per_warp * sizeof(int32_t), 0,
-                   (size_t)s->map_words * sizeof(int32_t), (size_t)warps));
+                   (size_t)s->sl.zero_words * sizeof(int32_t), (size_t)warps));
   SCK(cudaMalloc((void**)&s->d_arena, (size_t)c.arena_bytes));
   SCK(cudaMalloc((void**)&s->d_sctl, sizeof(ServeCtl)));
   SCK(cudaMemset(s->d_sctl, 0, sizeof(ServeCtl)));

@@ -105,7 +105,9 @@ typedef struct mbe_params {
                            /*   split into parts of range_chunk P candidates; each part  */
                            /*   redoes the root's set-up and pushes, at the first level, */
                            /*   only the candidates whose id hashes to it (earlier parts */
-                           /*   act as Q).  <= 0 = never (default)                       */
+                           /*   act as Q).  <= 0 = never (default).  In a launch with   */
+                           /*   two scratch tiers a listed big root's parts run on the   */
+                           /*   big warps only                                           */
   int32_t range_chunk;     /* P candidates per part (0 = default 64)                     */
   int32_t eager_share;     /* split_mode 0: a child of the counts tier (|L| > bitmap_max_l) */
                            /*   that passes the split test is shared out even while no  */
@@ -116,13 +118,23 @@ typedef struct mbe_params {
                            /*   other warps are sized for this bound.  0 = two tiers only */
                            /*   when one layout for every warp does not fit the device    */
                            /*   (the bound is then chosen); needs split_mode 0, and turns */
-                           /*   root_split_size and range_split_work off                  */
+                           /*   root_split_size off                                       */
   int32_t big_warps;       /* warps of that pool (0 = as many as fit, at most half)      */
-  int32_t reserved_p;      /* zero */
+  int32_t l2_window;       /* 0 = default: the launch keeps the graph's U -> V lists in a  */
+                           /*   persisting L2 access-policy window (as much as the       */
+                           /*   device's persisting L2 holds); < 0 = no window            */
   int64_t time_limit_ns;   /* a launch that runs longer than this gives up: every warp    */
                            /*   leaves at its next check (task boundary, counts-tier step,*/
                            /*   or every 4,096 bitmap-tier steps) and the call returns    */
                            /*   MBE_ERR_TIMEOUT; the result is then incomplete.  0 = none */
+  int32_t touch_scan;      /* how counting passes find first touches when the per-warp    */
+                           /*   shared-memory bitmap does not fit (|V| above ~114k):      */
+                           /*   0 = default: a large pass sets bits in a global bitmap    */
+                           /*   with fire-and-forget atomics and scans it, a small one    */
+                           /*   waits for each atomic's old value; 1 = every pass scans,  */
+                           /*   with the shared bitmap off; -1 = never scan.  Results do  */
+                           /*   not depend on it                                          */
+  int32_t reserved_q;      /* zero */
 } mbe_params;
 
 typedef struct mbe_result {

@@ -37,13 +37,26 @@ def test_tiny_vs_brute_force(gm, seed, shape):
 @pytest.mark.parametrize("bitmap", [-1, 32, 64, 0])
 @pytest.mark.parametrize("prune", [1, 0])
 @pytest.mark.parametrize("split", [(20, 1500), (1, 1), (1 << 30, 1 << 30)])
-def test_params_do_not_change_result(gm, bitmap, prune, split):
+@pytest.mark.parametrize("touch_scan", [0, 1])
+def test_params_do_not_change_result(gm, bitmap, prune, split, touch_scan):
+    # touch_scan 1: every counting pass collects its first touches from the
+    # global bitmap (the path graphs with |V| above ~114k take).
     ro, co, nU = planted(300, 200, blocks=6, seed=3, bsize=14)
     want = oracle.gmbe(ro, co, nU)
     r = run(gm, ro, co, nU, bitmap_max_l=bitmap, prune=prune, bound_height=split[0],
-            bound_size=split[1])
+            bound_size=split[1], touch_scan=touch_scan)
     assert r.status == 0
     assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_touch_scan_on_hub_graphs(gm, seed):
+    # Counts-tier roots (|L| = 300) with every first touch from the global bitmap.
+    ro, co, nU = hub_graph(seed)
+    want = oracle.gmbe(ro, co, nU)
+    for ts in (1, -1):
+        r = run(gm, ro, co, nU, touch_scan=ts)
+        assert (r.count, r.set_hash) == (want.count, want.set_hash)
 
 
 @pytest.mark.parametrize("uvtrans,order", [(0, 0), (0, 1), (0, 2), (1, 1), (2, 2), (1, 3)])

@@ -97,3 +97,21 @@ def test_two_tiers_need_split_mode_0(gm):
         with pytest.raises(gm.MBEError) as ei:
             G.enumerate(big_two_hop=10, split_mode=1)
     assert ei.value.name == "MBE_ERR_INVALID"
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("work,chunk", [(1, 1), (50, 4), (400, 64)])
+def test_two_tiers_with_root_parts(gm, name, make, work, chunk):
+    # Roots split into parts: a listed big root's parts go through the part
+    # records that only big warps claim, the other roots' parts through the
+    # common queue.  Thresholds this low split nearly every root.
+    ro, co, nU = make()
+    want = oracle.gmbe(ro, co, nU)
+    with gm.Graph.from_csr(ro, co, nU, uvtrans=1) as G:
+        for big_warps in (0, 2):
+            r = G.enumerate(big_two_hop=64, big_warps=big_warps, range_split_work=work,
+                            range_chunk=chunk, wait_limit_ns=WAIT)
+            assert r.status == 0
+            assert (r.count, r.set_hash) == (want.count, want.set_hash)
+            if chunk == 1:
+                assert r.tasks_split > 0

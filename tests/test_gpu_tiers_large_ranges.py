@@ -39,3 +39,24 @@ def test_large_config_root_ranges_match_oracle(gm):
                             wait_limit_ns=60 * 10**9)
             assert r.status == 0
             assert (r.count, f"{r.set_hash:#018x}") == (rg["count"], rg["set_hash"]), rg
+
+
+SHARDS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "large_shards.json")
+
+
+def test_large_config_root_shards_match_oracle(gm):
+    # Interleaved 1/20000 root shards of the large graph (the heaviest roots
+    # at the top of the degree order included) against the oracle's count
+    # and set hash in tests/golden/large_shards.json
+    # (tests/golden/make_large_shards.py).  The whole launch plan runs: two
+    # scratch tiers, big-root parts.  The device build orders roots exactly as
+    # the host build does, so the same shards hold the same roots.
+    with open(SHARDS) as f:
+        d = json.load(f)
+    g = gm.config_graph("large")
+    with gm.Graph.build_on_device(g.row_off, g.col, g.nU, uvtrans=1, order=1) as G:
+        for sh in d["shards"]:
+            r = G.enumerate(shard_count=sh["shard_count"], shard_index=sh["shard_index"],
+                            wait_limit_ns=600 * 10**9, time_limit_ns=900 * 10**9)
+            assert r.status == 0
+            assert (r.count, f"{r.set_hash:#018x}") == (sh["count"], sh["set_hash"]), sh
