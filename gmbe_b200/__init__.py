@@ -63,7 +63,7 @@ class Params(C.Structure):
                 ("eager_share", C.c_int32), ("big_two_hop", C.c_int32),
                 ("big_warps", C.c_int32), ("l2_window", C.c_int32),
                 ("time_limit_ns", C.c_int64), ("touch_scan", C.c_int32),
-                ("reserved_q", C.c_int32)]
+                ("slot_records", C.c_int32)]
 
 
 class Result(C.Structure):

@@ -187,7 +187,7 @@ ScratchLayout make_layout(int32_t nV, int32_t capC, int32_t capL, int32_t capS) 
 int choose_tiers(int32_t nV, int32_t n_roots, const int64_t* S, const int32_t* D,
                  const int32_t* roots, int warps, uint64_t budget, int64_t force_bound,
                  int32_t force_big, TierChoice* out, std::vector<int32_t>* list,
-                 std::vector<uint8_t>* flags) {
+                 std::vector<uint8_t>* flags, bool pool_for_parts) {
   *out = TierChoice();
   list->clear();
   flags->clear();
@@ -251,9 +251,9 @@ int choose_tiers(int32_t nV, int32_t n_roots, const int64_t* S, const int32_t* D
                      warps, (long long)T, small_b * (double)warps / 1e9, budget / 1e9);
   const uint64_t extra = full_b > small_b ? full_b - small_b : 0;
   const int64_t fit = extra ? (int64_t)((budget - small_b * (uint64_t)warps) / extra) : warps;
-  int64_t n_big = force_big > 0
-                      ? force_big
-                      : std::min<int64_t>({(int64_t)list->size(), fit, (int64_t)warps / 2});
+  const int64_t want = pool_for_parts ? (int64_t)warps : (int64_t)list->size();
+  int64_t n_big = force_big > 0 ? force_big
+                                : std::min<int64_t>({want, fit, (int64_t)warps / 2});
   n_big = std::min<int64_t>(n_big, warps);
   if (n_big < 1 || n_big > fit)
     return set_error(MBE_ERR_NOMEM, "%lld warps for the largest roots (%.2f GB each) do not fit",
@@ -351,6 +351,16 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
     ws.nslot = nslot;
     ++ws.gen;
   }
+  if (!ws.big_slots) {
+    // Large slots: children with more candidates than a regular slot holds
+    // (graphs whose candidate sets reach hundreds of thousands) can still go
+    // to idle warps.  128 x 4 MiB = 512 MiB.
+    const int32_t nbig = 128;
+    CK(cudaMalloc((void**)&ws.big_slots, sizeof(int32_t) * (size_t)kBigSlotWords * nbig));
+    CK(cudaMalloc((void**)&ws.big_slot_bits, sizeof(uint32_t) * (size_t)(nbig / 32)));
+    ws.nbig_slot = nbig;
+    ++ws.gen;
+  }
   if (plan->blocks > ws.exit_cap) {
     cudaFree(ws.exit_ns);
     ws.exit_ns = nullptr;
@@ -372,6 +382,7 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.idle_ns_limit = prm.wait_limit_ns > 0 ? prm.wait_limit_ns : 600LL * 1000000000LL;
   ep.time_limit_ns = std::max<int64_t>(prm.time_limit_ns, 0);
   ep.touch_scan = prm.touch_scan > 0 ? 1 : (prm.touch_scan < 0 ? -1 : 0);
+  ep.slot_records = std::max(prm.slot_records, 0);
   ep.record_exit = prm.sm_timing ? 1 : 0;
   ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
   // Heavy roots split into vertex tuples (sub-problem sharing mode only).
@@ -383,13 +394,21 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.n_big_warps = n_big;
   ep.big_sl = big_sl;
   if (n_big > 0) {
-    // Vertex-tuple children could need the big tier: off.  Root parts stay
-    // available (a big root's parts go to big warps only).
+    // Vertex-tuple children could need the big tier: off.  Heavy roots are
+    // split into parts by default (a big root's parts run on big warps only):
+    // in graphs whose worst roots do not fit every warp, single roots
+    // otherwise run for most of a launch on one warp.
     ep.root_split = 0;
+    if (prm.range_split_work == 0 && prm.split_mode != 1) ep.range_work = kRangeWorkTiersDefault;
   }
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;
   plan->pool.nslot = prm.split_mode == 1 ? 0 : ws.nslot;
+  plan->pool.big = ws.big_slots;
+  plan->pool.big_bits = ws.big_slot_bits;
+  plan->pool.nbig = prm.split_mode == 1 ? 0 : ws.nbig_slot;
+  plan->pool.import_cap = plan->sl.capC;  // the small tier's (every warp has at least this)
+  plan->pool.pad = 0;
   return MBE_OK;
 }
 
@@ -424,6 +443,7 @@ int engine_enqueue(Workspace& ws, LaunchPlan* plan, const DevGraph* d_graphs,
   CK(cudaMemsetAsync(ws.ctl, 0, sizeof(EnumCtl), st));
   CK(cudaMemsetAsync(ws.q_seq, 0, sizeof(unsigned long long) * (size_t)ws.q_cap, st));
   CK(cudaMemsetAsync(ws.slot_bits, 0, sizeof(uint32_t) * (size_t)(ws.nslot / 32), st));
+  CK(cudaMemsetAsync(ws.big_slot_bits, 0, sizeof(uint32_t) * (size_t)(ws.nbig_slot / 32), st));
   CK(cudaMemsetAsync(d_gres, 0, 3 * sizeof(unsigned long long) * (size_t)n_graphs, st));
   if (ev0) CK(cudaEventRecord(ev0, st));
   auto* kernel = plan->ep.n_big_warps > 0 ? mbe_enum_kernel_tiers : mbe_enum_kernel;
@@ -639,8 +659,9 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t rb, int32_t re, 
     roots[(size_t)k] = v;
   }
   TierChoice ch;
+  const bool parts = prm.split_mode != 1 && prm.range_split_work >= 0;
   if ((rc = choose_tiers(nV, n_roots, S.data(), D.data(), roots.data(), warps, budget,
-                         prm.big_two_hop, prm.big_warps, &ch, list, flags)))
+                         prm.big_two_hop, prm.big_warps, &ch, list, flags, parts)))
     return rc;
   if (ch.n_big > 0 && prm.split_mode == 1)
     return set_error(MBE_ERR_INVALID, "split_mode 1 needs one scratch tier for every warp");

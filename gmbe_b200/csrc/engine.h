@@ -28,6 +28,9 @@ struct Workspace {
   int32_t* slots = nullptr;  // exported bitmap sub-problems
   uint32_t* slot_bits = nullptr;
   int32_t nslot = 0;
+  int32_t* big_slots = nullptr;  // large ones (kBigSlotWords words each)
+  uint32_t* big_slot_bits = nullptr;
+  int32_t nbig_slot = 0;
   // Single-graph launch descriptors.
   DevGraph* d_graph1 = nullptr;
   long long* d_prefix1 = nullptr;

@@ -107,12 +107,20 @@ struct ScratchLayout {
   int64_t zero_words;
 };
 
-// Slots for bitmap sub-problems handed to idle warps.
+// Slots for bitmap sub-problems handed to idle warps.  Slot s < nslot is
+// a regular slot; s >= nslot is large slot s - nslot, for children with more
+// candidates than a regular slot holds.
 struct SlotPool {
-  int32_t* slots;  // nslot x 32768 int32 words
-  uint32_t* bits;  // occupancy, nslot / 32 words, zero at launch
-  int32_t nslot;   // multiple of 32; 0 disables export
+  int32_t* slots;     // nslot x 32768 int32 words
+  uint32_t* bits;     // occupancy, nslot / 32 words, zero at launch
+  int32_t nslot;      // multiple of 32; 0 disables export
+  int32_t nbig;       // large slots: multiple of 32 (0: none)
+  int32_t* big;       // nbig x kBigSlotWords int32 words
+  uint32_t* big_bits; // their occupancy, nbig / 32 words, zero at launch
+  int32_t import_cap; // most candidates any warp of the launch can take in
+  int32_t pad;
 };
+constexpr int kBigSlotWords = 1 << 20;  // 4 MiB
 
 // Serving.  Every resident graph is one block of the device arena, aligned to
 // 1 << kServeBlockShift bytes and named by its block index: this header, then
@@ -160,7 +168,7 @@ struct EnumParams {
   int64_t idle_ns_limit;      // nanoseconds a warp may idle waiting for work
   int64_t time_limit_ns;      // > 0: the launch gives up after this long (kStDeadline)
   int32_t touch_scan;         // 0 auto, 1 always scan the global touch bitmap, -1 never
-  int32_t pad_ts;
+  int32_t slot_records;       // > 0: regular slots take children of at most this many records
   int32_t record_exit;        // -p
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)

@@ -101,6 +101,10 @@ struct Warp {
   int32_t* slots;        // exported bitmap sub-problems (nslot x slot_words)
   uint32_t* slot_bits;   // slot occupancy
   int nslot;
+  int32_t* bigslots;     // large slots (nbig x kBigSlotWords)
+  uint32_t* big_bits;
+  int nbig;
+  int import_cap;        // most candidates any warp of the launch can take in
   int32_t* base;
   const DevGraph* graphs;  // every graph of the launch
   const DevGraph* gp;      // graph of the task being run
@@ -305,6 +309,9 @@ constexpr int kSlotRec = kSlotLid + 32 * 4;
 __host__ __device__ constexpr int slot_cap(int K) {
   return ((kSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
 }
+__host__ __device__ constexpr int big_slot_cap(int K) {
+  return ((kBigSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
+}
 static_assert(slot_cap(1) == kSlotMaxRecords && slot_cap(1) >= slot_cap(2) &&
                   slot_cap(2) >= slot_cap(4) && kSlotWords == kSlotWordsHost,
               "host view of the slot size");
@@ -313,17 +320,17 @@ __device__ __forceinline__ uint64_t* slot_subkey(int32_t* sp, int K, int nsub) {
   return reinterpret_cast<uint64_t*>(sp + kSlotRec + ((nsub * (K + 1) + 1) & ~1));
 }
 
-// Claims a free slot (lane 0); -1 if none.
-__device__ int slot_alloc(Warp& W) {
-  const int nw = W.nslot >> 5;
+// Claims a free slot of an occupancy bitmap of n slots (lane 0); -1 if none.
+__device__ int bits_alloc(uint32_t* bits, int n) {
+  const int nw = n >> 5;
   if (nw == 0) return -1;
   int start = (int)(((blockIdx.x * 32u + (threadIdx.x >> 5)) * 2654435761u) % (unsigned)nw);
   for (int t = 0; t < nw; ++t) {
     int wi = (start + t) % nw;
-    unsigned cur = *(volatile unsigned*)&W.slot_bits[wi];
+    unsigned cur = *(volatile unsigned*)&bits[wi];
     while (cur != 0xffffffffu) {
       int b = __ffs(~cur) - 1;
-      unsigned old = atomicOr(&W.slot_bits[wi], 1u << b);
+      unsigned old = atomicOr(&bits[wi], 1u << b);
       if (!(old & (1u << b))) return wi * 32 + b;
       cur = old | (1u << b);
     }
@@ -331,7 +338,41 @@ __device__ int slot_alloc(Warp& W) {
   return -1;
 }
 
-__device__ void slot_free(Warp& W, int s) { atomicAnd(&W.slot_bits[s >> 5], ~(1u << (s & 31))); }
+// A regular slot (lane 0); -1 if none.
+__device__ int slot_alloc(Warp& W) { return bits_alloc(W.slot_bits, W.nslot); }
+
+// A slot for a sub-problem of nsub candidates with K-word masks (lane 0): a
+// regular one when it fits, else a large one if some warp of every tier can
+// take it in; -1 if none.
+__device__ __forceinline__ bool regular_fits(const Warp& W, int nsub, int K) {
+  return nsub <= slot_cap(K) && (W.p.slot_records <= 0 || nsub <= W.p.slot_records);
+}
+
+__device__ int slot_alloc_for(Warp& W, int nsub, int K) {
+  if (regular_fits(W, nsub, K)) return slot_alloc(W);
+  if (nsub > big_slot_cap(K) || nsub > W.import_cap) return -1;
+  const int b = bits_alloc(W.big_bits, W.nbig);
+  return b < 0 ? -1 : W.nslot + b;
+}
+
+// Whether a child of nsub candidates can be exported at all.
+__device__ __forceinline__ bool slot_fits(const Warp& W, int nsub, int K) {
+  return regular_fits(W, nsub, K) ||
+         (W.nbig > 0 && nsub <= big_slot_cap(K) && nsub <= W.import_cap);
+}
+
+__device__ __forceinline__ int32_t* slot_ptr(const Warp& W, int s) {
+  return s < W.nslot ? W.slots + (size_t)s * kSlotWords
+                     : W.bigslots + (size_t)(s - W.nslot) * kBigSlotWords;
+}
+
+__device__ void slot_free(Warp& W, int s) {
+  if (s < W.nslot) atomicAnd(&W.slot_bits[s >> 5], ~(1u << (s & 31)));
+  else {
+    const int b = s - W.nslot;
+    atomicAnd(&W.big_bits[b >> 5], ~(1u << (b & 31)));
+  }
+}
 
 __device__ bool queue_push_one(Warp& W, const Task& t);
 
@@ -405,14 +446,14 @@ __device__ void slot_header(int32_t* sp, int K, int nsub, int nq, const uint32_t
 template <int K>
 __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, int nchild,
                               int nbefore, const uint32_t* Ln, int kn, uint64_t sR, uint64_t nR) {
-  if (nchild > slot_cap(K) || !should_export(W, nchild - nbefore, kn))
+  if (!slot_fits(W, nchild, K) || !should_export(W, nchild - nbefore, kn))
     return false;
   const int lane = (int)lane_id();
-  int slot = lane == 0 ? slot_alloc(W) : 0;
+  int slot = lane == 0 ? slot_alloc_for(W, nchild, K) : 0;
   slot = __shfl_sync(0xffffffffu, slot, 0);
   if (slot < 0) return false;
   constexpr int RS = K + 1;
-  int32_t* sp = W.slots + (size_t)slot * kSlotWords;
+  int32_t* sp = slot_ptr(W, slot);
   uint32_t* rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
   uint64_t* key = slot_subkey(sp, K, nchild);
   uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
@@ -729,7 +770,7 @@ __device__ void tier2(Warp& W, int n, int nsub, int nq, int nend, uint64_t sR0, 
 // records of its next owner.
 __device__ void tier2_from_slot(Warp& W, int slot) {
   const int lane = (int)lane_id();
-  int32_t* sp = W.slots + (size_t)slot * kSlotWords;
+  int32_t* sp = slot_ptr(W, slot);
   volatile const int32_t* vh = sp;
   const int K = vh[0];
   const int nsub = vh[1];
@@ -1135,14 +1176,14 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
     // big enough by GMBE's split test, else this warp's scratch.
     const int K = words_k(n), RS = K + 1;
     int slot = -1;
-    if (ncand <= slot_cap(K) && should_export(W, ncand - nqc, n, W.p.eager_share != 0)) {
-      slot = lane == 0 ? slot_alloc(W) : 0;
+    if (slot_fits(W, ncand, K) && should_export(W, ncand - nqc, n, W.p.eager_share != 0)) {
+      slot = lane == 0 ? slot_alloc_for(W, ncand, K) : 0;
       slot = __shfl_sync(kFull, slot, 0);
     }
     uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
     int32_t* sp = nullptr;
     if (slot >= 0) {
-      sp = W.slots + (size_t)slot * kSlotWords;
+      sp = slot_ptr(W, slot);
       rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
       subkey = slot_subkey(sp, K, ncand);
       uint64_t* lk = reinterpret_cast<uint64_t*>(sp + kSlotLkey);
@@ -2003,6 +2044,7 @@ __device__ void run_task(Warp& W, const Task& t) {
       int32_t* fill = W.A(W.sl.fill);
       int32_t* cadj = W.A(W.sl.cadj);
       int32_t* sidx = W.A(W.sl.sidx);
+      int32_t* ent = W.A(W.sl.ent);  // free until the first sparse push
       for (int l = lane; l < nL; l += 32) llevel[l] = 0;
       // aadj: L row -> C index (or -1 for R), rows sized by degree
       flat_rows(
@@ -2017,6 +2059,7 @@ __device__ void run_task(Warp& W, const Task& t) {
             int u = L[r];
             int off = aoff[r] + (pos - g.rev_off[u]);
             aadj[off] = map[__ldg(g.rev_col + pos)] - 1;
+            ent[off] = r;  // the entry's row, for the transpose below
           });
       // coff = exclusive scan of the initial counts; fill = 0; sidx = -1
       {
@@ -2036,20 +2079,25 @@ __device__ void run_task(Warp& W, const Task& t) {
         if (lane == 0) coff[nC] = run;
       }
       __syncwarp();
-      // cadj: C index -> L positions
-      flat_rows(
-          nL,
-          [&](int r, int& beg, int& len) {
-            beg = aoff[r];
-            len = aoff[r + 1] - beg;
-          },
-          [&](bool valid, int r, int pos) {
-            if (!valid) return;
-            int p = aadj[pos];
-            if (p < 0) return;
-            int s = atomicAdd(&fill[p], 1);
-            cadj[coff[p] + s] = r;
-          });
+      // cadj: C index -> L positions.  A linear pass over the entries: each
+      // lane has four slot reservations in flight before it uses any.
+      {
+        const int S = aoff[nL];
+        for (int j0 = 0; j0 < S; j0 += 128) {
+          int pp[4], rr[4], ss[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int j = j0 + k * 32 + lane;
+            pp[k] = j < S ? aadj[j] : -1;
+            rr[k] = j < S ? ent[j] : 0;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) ss[k] = pp[k] >= 0 ? atomicAdd(&fill[pp[k]], 1) : 0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (pp[k] >= 0) cadj[coff[pp[k]] + ss[k]] = rr[k];
+        }
+      }
       __syncwarp();
       // fill doubles as the sparse push's child-count array: back to zero.
       for (int i = lane; i < nC; i += 32) fill[i] = 0;
@@ -2163,6 +2211,10 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
   W.q_tasks = q_tasks;
   W.q_seq = q_seq;
   W.slots = pool.slots;
+  W.bigslots = pool.big;
+  W.big_bits = pool.big_bits;
+  W.nbig = pool.nbig;
+  W.import_cap = pool.import_cap;
   W.slot_bits = pool.bits;
   W.nslot = pool.nslot;
   if (!kTiers)

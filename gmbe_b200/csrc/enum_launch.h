@@ -47,6 +47,9 @@ constexpr int32_t kShareMinWorkDefault = 256;
 constexpr int32_t kServeShareMinWorkDefault = 64;
 // P candidates per part of a root split into parts.
 constexpr int32_t kRangeChunkDefault = 64;
+// |P|*|C| above which a root of a two-tier launch (a graph whose worst roots
+// do not fit every warp) is split into parts unless the caller says otherwise.
+constexpr int32_t kRangeWorkTiersDefault = 1000000000;
 
 
 // Per-warp scratch layout for the given capacities.

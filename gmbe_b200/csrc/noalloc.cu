@@ -220,6 +220,7 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   ep.time_limit_ns = prm.time_limit_ns > 0 ? prm.time_limit_ns : 0;
   ep.record_exit = 0;
   SlotPool none;
+  memset(&none, 0, sizeof(none));
   none.slots = nullptr;
   none.bits = nullptr;
   none.nslot = 0;  // no sub-problem export out of the static pool

@@ -216,6 +216,7 @@ int launch(mbe_server* s) {
   if (s->nslot)
     SCK(cudaMemsetAsync(s->d_slot_bits, 0, sizeof(uint32_t) * (size_t)(s->nslot / 32), s->s_run));
   SlotPool pool;
+  memset(&pool, 0, sizeof(pool));  // no large slots in a server
   pool.slots = s->d_slots;
   pool.bits = s->d_slot_bits;
   pool.nslot = s->nslot;

@@ -33,9 +33,12 @@ struct TierChoice {
 // for the largest root.  The small tier holds any exported sub-problem.
 // Returns MBE_OK, MBE_ERR_CAPACITY (a root above 2^30 two-hop entries) or
 // MBE_ERR_NOMEM (the small tier or the big warps do not fit).
+// pool_for_parts: the listed roots may be split into parts that only big
+// warps run, so the big pool is not limited to the number of listed roots
+// (as many as fit, at most half of the warps).
 int choose_tiers(int32_t nV, int32_t n_roots, const int64_t* S, const int32_t* D,
                  const int32_t* roots, int warps, uint64_t budget, int64_t force_bound,
                  int32_t force_big, TierChoice* out, std::vector<int32_t>* list,
-                 std::vector<uint8_t>* flags);
+                 std::vector<uint8_t>* flags, bool pool_for_parts = false);
 
 }  // namespace gmbe

@@ -232,3 +232,19 @@ def test_shards_match_oracle_and_add_up(gm, world):
             tot_c += r.count
             tot_h = (tot_h + r.set_hash) % (1 << 64)
     assert (full.count, full.set_hash) == (tot_c, tot_h)
+
+
+@pytest.mark.parametrize("slot_records", [8, 64])
+@pytest.mark.parametrize("case", ["planted", "hub", "dense"])
+def test_large_export_slots(gm, slot_records, case):
+    # Shared-out children with more than slot_records candidates go through
+    # the 4 MiB slots (on the large graph, children of hundreds of thousands
+    # of candidates do); share_min_work 1 shares nearly every child.
+    ro, co, nU = {"planted": lambda: planted(300, 200, blocks=6, seed=3, bsize=14),
+                  "hub": lambda: hub_graph(3),
+                  "dense": lambda: random_bipartite(40, 60, 0.35, 9)}[case]()
+    want = oracle.gmbe(ro, co, nU)
+    for params in (dict(), dict(bitmap_max_l=64), dict(big_two_hop=64)):
+        r = run(gm, ro, co, nU, slot_records=slot_records, share_min_work=1, **params)
+        assert r.status == 0
+        assert (r.count, r.set_hash) == (want.count, want.set_hash), params
