@@ -407,7 +407,10 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   plan->pool.big = ws.big_slots;
   plan->pool.big_bits = ws.big_slot_bits;
   plan->pool.nbig = prm.split_mode == 1 ? 0 : ws.nbig_slot;
-  plan->pool.import_cap = plan->sl.capC;  // the small tier's (every warp has at least this)
+  // The small tier's capacities: every warp has at least these.
+  plan->pool.import_cap = plan->sl.capC;
+  plan->pool.import_l = plan->sl.capL;
+  plan->pool.import_s = plan->sl.capS;
   plan->pool.pad = 0;
   return MBE_OK;
 }

@@ -118,6 +118,8 @@ struct SlotPool {
   int32_t* big;       // nbig x kBigSlotWords int32 words
   uint32_t* big_bits; // their occupancy, nbig / 32 words, zero at launch
   int32_t import_cap; // most candidates any warp of the launch can take in
+  int32_t import_l;   // most L vertices any warp can take in
+  int32_t import_s;   // largest two-hop multiset any warp can take in
   int32_t pad;
 };
 constexpr int kBigSlotWords = 1 << 20;  // 4 MiB

@@ -105,6 +105,7 @@ struct Warp {
   uint32_t* big_bits;
   int nbig;
   int import_cap;        // most candidates any warp of the launch can take in
+  int import_l, import_s; // most L vertices / two-hop entries any warp can take in
   int32_t* base;
   const DevGraph* graphs;  // every graph of the launch
   const DevGraph* gp;      // graph of the task being run
@@ -420,12 +421,14 @@ __device__ bool should_export(Warp& W, int nP, int nL, bool eager = false) {
 }
 
 // Enqueues a filled slot as a task; false if the ring is full.
-__device__ bool slot_publish(Warp& W, int slot) {
+// kind 0: a bitmap sub-problem; kind 1: a counts-tier child (vertex lists).
+__device__ bool slot_publish(Warp& W, int slot, int kind = 0) {
   __syncwarp();
   __threadfence();
   Task t;
   t.v[0] = -2 - slot;
-  t.v[1] = t.v[2] = t.v[3] = -1;
+  t.v[1] = kind ? 1 : -1;
+  t.v[2] = t.v[3] = -1;
   t.graph = t.part = t.parts = t.pad = 0;
   return queue_push_one(W, t);
 }
@@ -1298,6 +1301,110 @@ __device__ __forceinline__ int t1_next_live(const int32_t* bound, const int32_t*
   return -1;
 }
 
+// Counts-tier child export.  A push at `level` of candidate x whose new L
+// (the `kept` rows, llevel == level) is too large for the bitmap tier
+// descends in place; when warps wait for work the child goes to one of them
+// instead, as vertex lists in a slot: L' = the kept rows' vertices, C' = the
+// candidates live below this level (bound > level) with 0 < count < kept,
+// in index order (those before x are its Q), and the R sum and size of the
+// push.  Every bound of C' is free at the child's first level (a bound above
+// `level` is FREE or TOUCHED there), so the importer starts from a clean
+// frame, and the child's levels leave this level's state as they found it:
+// the exporter pops x at once.  nbits holds the candidates the kept rows
+// meet (the bitmap of level + 1).  Slot: header of 16 words {|L'|, |C'|,
+// |Q'|, graph, sR (2 words), |R|}, then L' ids, then C' ids.
+constexpr int kFrameHdr = 16;
+
+// Whether a counts-tier child of `kept` rows (`kent` entries) may be shared
+// out now: slots exist, every warp has room for it, warps wait for work.
+__device__ __forceinline__ bool t1_export_wanted(Warp& W, int kept, long long kent) {
+  if (W.nslot == 0 && W.nbig == 0) return false;
+  if (kept > W.import_l || kent > (long long)W.import_s) return false;
+  return export_demand(W) != 0;
+}
+
+__device__ bool t1_try_export(Warp& W, const T1& t, int x, int level, int kept, long long kent,
+                              uint64_t sR, uint64_t nR, const uint32_t* nbits) {
+  const int lane = (int)lane_id();
+  const int32_t* bound = W.A(W.sl.bound);
+  const int32_t* ncnt = W.A(W.sl.ncnt);
+  const int32_t* cv = W.A(W.sl.cv);
+  const int32_t* coff = W.A(W.sl.coff);
+  const int32_t* cadj = W.A(W.sl.cadj);
+  const int32_t* llevel = W.A(W.sl.llevel);
+  const int cwords = (t.nC + 31) >> 5;
+  int m = 0, mq = 0;
+  for (int w0 = 0; w0 < cwords; w0 += 32) {
+    const int w = w0 + lane;
+    uint32_t b = w < cwords ? nbits[w] : 0u;
+    while (b) {
+      const int p = (w << 5) + __ffs(b) - 1;
+      if (bound[p] > level && ncnt[p] < kept) {
+        ++m;
+        mq += p < x;
+      }
+      b &= b - 1;
+    }
+  }
+  m = warp_sum(m);
+  mq = warp_sum(mq);
+  if (m == 0 || m > W.import_cap || !should_export(W, m - mq, kept)) return false;
+  const long long words = kFrameHdr + (long long)kept + m;
+  int slot = -1;
+  if (lane == 0) {
+    if (words <= kSlotWords) slot = slot_alloc(W);
+    if (slot < 0 && words <= kBigSlotWords) {
+      const int b = bits_alloc(W.big_bits, W.nbig);
+      if (b >= 0) slot = W.nslot + b;
+    }
+  }
+  slot = __shfl_sync(kFull, slot, 0);
+  if (slot < 0) return false;
+  int32_t* sp = slot_ptr(W, slot);
+  // L' ids: the kept rows, from x's row of cadj
+  int nl = 0;
+  for (int j0 = coff[x]; j0 < coff[x + 1]; j0 += 32) {
+    const int j = j0 + lane;
+    const int l = j < coff[x + 1] ? cadj[j] : 0;
+    const bool sel = j < coff[x + 1] && llevel[l] == level;
+    const unsigned bal = __ballot_sync(kFull, sel);
+    if (sel) sp[kFrameHdr + nl + __popc(bal & lanemask_lt())] = t.L[l];
+    nl += __popc(bal);
+  }
+  // C' ids in index order: lane k takes word k of each round
+  int32_t* cdst = sp + kFrameHdr + kept;
+  int o = 0;
+  for (int w0 = 0; w0 < cwords; w0 += 32) {
+    const int w = w0 + lane;
+    uint32_t b = w < cwords ? nbits[w] : 0u;
+    uint32_t keep = 0u;
+    for (uint32_t bb = b; bb; bb &= bb - 1) {
+      const int bit = __ffs(bb) - 1;
+      const int p = (w << 5) + bit;
+      if (bound[p] > level && ncnt[p] < kept) keep |= 1u << bit;
+    }
+    int tot;
+    int at = o + warp_excl_scan(__popc(keep), &tot);
+    for (; keep; keep &= keep - 1) cdst[at++] = cv[(w << 5) + __ffs(keep) - 1];
+    o += tot;
+  }
+  if (lane == 0) {
+    sp[0] = kept;
+    sp[1] = m;
+    sp[2] = mq;
+    sp[3] = W.gid;
+    *reinterpret_cast<uint64_t*>(sp + 4) = sR;
+    sp[6] = (int32_t)nR;
+  }
+  if (slot_publish(W, slot, 1)) {
+    W.splits += 1;
+    return true;
+  }
+  if (lane == 0) slot_free(W, slot);
+  __syncwarp();
+  return false;
+}
+
 __device__ void tier1_run(Warp& W, const T1& t) {
   const int lane = (int)lane_id();
   int32_t* llevel = W.A(W.sl.llevel);
@@ -1426,22 +1533,45 @@ __device__ void tier1_run(Warp& W, const T1& t) {
         if (kept <= t2max) {
           t1_handoff(W, t, cur, level, kept, sR, nR);
         } else {
-          if (lane == 0) {
-            stack[level - 1] = cur;
-            stack[level] = cur + 1;
-            lent[level] = (int32_t)kent;
-          }
           uint32_t* nbits = level_bits(W, level + 1);
-          if (nbits) {
+          // The candidates the kept rows meet, as a bitmap: the next level's
+          // own one, or (deeper levels) the warp's global touch bitmap, built
+          // only when the child may be shared out.
+          uint32_t* cbits = nbits;
+          const bool want = t1_export_wanted(W, kept, kent);
+          if (!cbits && want) cbits = W.gseen;
+          if (cbits) {
             t1_rows_of(W, cur, level, [&](bool valid, int, int pos) {
               if (!valid) return;
               const int p = aadj[pos];
-              if (p >= 0) atomicOr(&nbits[p >> 5], 1u << (p & 31));
+              if (p >= 0) atomicOr(&cbits[p >> 5], 1u << (p & 31));
             });
+            __threadfence_block();
+            __syncwarp();
           }
-          __syncwarp();
-          ++level;
-          continue;
+          const bool exported =
+              want && cbits && t1_try_export(W, t, cur, level, kept, kent, sR, nR, cbits);
+          if (cbits && (exported || cbits != nbits)) {
+            // back to clear: a shared-out child's level bitmap, or the touch bitmap
+            t1_rows_of(W, cur, level, [&](bool valid, int, int pos) {
+              if (!valid) return;
+              const int p = aadj[pos];
+              if (p >= 0) cbits[p >> 5] = 0u;
+            });
+            __syncwarp();
+          }
+          if (exported) {
+            // shared out: pop x here
+          } else {
+            if (lane == 0) {
+              stack[level - 1] = cur;
+              stack[level] = cur + 1;
+              lent[level] = (int32_t)kent;
+            }
+            __syncwarp();
+            ++level;
+            continue;
+          }
         }
       }
       if (lane == 0) stack[level - 1] = cur + 1;
@@ -1467,6 +1597,140 @@ __device__ void tier1_run(Warp& W, const T1& t) {
       }
     }
   }
+}
+
+// Runs a counts-tier child exported by t1_try_export: the frame is rebuilt
+// from the vertex lists (local adjacency from the graph's U -> V rows, the
+// counts of each candidate inside L'), then the counts tier runs it from its
+// first level.  The child's own biclique was counted by the exporter.
+__device__ void tier1_from_slot(Warp& W, int slot) {
+  const int lane = (int)lane_id();
+  int32_t* sp = slot_ptr(W, slot);
+  volatile const int32_t* vh = sp;
+  const int n = vh[0], m = vh[1], nq = vh[2];
+  const int32_t gid = vh[3];
+  const uint64_t sR = (uint64_t)(uint32_t)vh[4] | ((uint64_t)(uint32_t)vh[5] << 32);
+  const uint64_t nR = (uint32_t)vh[6];
+  int32_t* lv = W.A(W.sl.lv);
+  int32_t* cv = W.A(W.sl.cv);
+  const bool fits = n <= W.sl.capL && m <= W.sl.capC;
+  if (fits) {
+    const unsigned* src = reinterpret_cast<const unsigned*>(sp + kFrameHdr);
+    for (int i = lane; i < n; i += 32) lv[i] = (int32_t)__ldcg(src + i);
+    for (int i = lane; i < m; i += 32) cv[i] = (int32_t)__ldcg(src + n + i);
+  }
+  __syncwarp();
+  if (lane == 0) slot_free(W, slot);
+  __syncwarp();
+  if (!fits) {
+    set_status(W.ctl, kStCapacity, ((unsigned long long)4 << 32) | (unsigned)m);
+    return;
+  }
+  W.gid = gid;
+  W.gp = graph_at(W, gid);
+  const DevGraph& g = *W.gp;
+  int32_t* map = W.A(W.sl.map);
+  int32_t* aoff = W.A(W.sl.aoff);
+  int32_t* aadj = W.A(W.sl.aadj);
+  int32_t* ent = W.A(W.sl.ent);
+  int32_t* ncnt = W.A(W.sl.ncnt);
+  int32_t* bound = W.A(W.sl.bound);
+  int32_t* coff = W.A(W.sl.coff);
+  int32_t* fill = W.A(W.sl.fill);
+  int32_t* cadj = W.A(W.sl.cadj);
+  int32_t* sidx = W.A(W.sl.sidx);
+  int32_t* llevel = W.A(W.sl.llevel);
+  uint64_t* ckey = W.A64(W.sl.ckey);
+  uint64_t t0 = globaltimer_ns();
+  int run = 0;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int l = c0 + lane;
+    const int d = l < n ? g.rev_off[lv[l] + 1] - g.rev_off[lv[l]] : 0;
+    int tot;
+    const int ex = warp_excl_scan(d, &tot);
+    if (l < n) aoff[l] = run + ex;
+    run += tot;
+  }
+  if (lane == 0) aoff[n] = run;
+  if (run > W.sl.capS) {
+    set_status(W.ctl, kStCapacity, ((unsigned long long)5 << 32) | (unsigned)run);
+    return;
+  }
+  for (int i = lane; i < m; i += 32) {
+    map[cv[i]] = i + 1;
+    ncnt[i] = 0;
+    bound[i] = kFree;
+    fill[i] = 0;
+    sidx[i] = -1;
+    ckey[i] = g.vkey[cv[i]];
+  }
+  for (int l = lane; l < n; l += 32) llevel[l] = 0;
+  __threadfence_block();
+  __syncwarp();
+  flat_rows(
+      n,
+      [&](int r, int& beg, int& len) {
+        const int u = lv[r];
+        beg = g.rev_off[u];
+        len = g.rev_off[u + 1] - beg;
+      },
+      [&](bool valid, int r, int pos) {
+        if (!valid) return;
+        const int u = lv[r];
+        const int off = aoff[r] + (pos - g.rev_off[u]);
+        const int p = map[__ldg(g.rev_col + pos)] - 1;
+        aadj[off] = p;
+        ent[off] = r;
+        if (p >= 0) atomicAdd(&ncnt[p], 1);
+      });
+  __threadfence_block();
+  __syncwarp();
+  {
+    int acc = 0;
+    for (int c0 = 0; c0 < m; c0 += 32) {
+      const int i = c0 + lane;
+      const int c = i < m ? ncnt[i] : 0;
+      int tot;
+      const int ex = warp_excl_scan(c, &tot);
+      if (i < m) coff[i] = acc + ex;
+      acc += tot;
+    }
+    if (lane == 0) coff[m] = acc;
+  }
+  __syncwarp();
+  for (int j0 = 0; j0 < run; j0 += 128) {
+    int pp[4], rr[4], ss[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int j = j0 + k * 32 + lane;
+      pp[k] = j < run ? aadj[j] : -1;
+      rr[k] = j < run ? ent[j] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ss[k] = pp[k] >= 0 ? atomicAdd(&fill[pp[k]], 1) : 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (pp[k] >= 0) cadj[coff[pp[k]] + ss[k]] = rr[k];
+  }
+  __syncwarp();
+  for (int i = lane; i < m; i += 32) fill[i] = 0;
+  __syncwarp();
+  T1 t1;
+  t1.L = lv;
+  t1.nL = n;
+  t1.nC = m;
+  t1.nq = nq;
+  t1.nend = m;
+  t1.sRtask = sR;
+  t1.nRtask = nR;
+  const uint64_t t1s = globaltimer_ns();
+  const uint64_t t2_before = W.ns_t2;
+  tier1_run(W, t1);
+  W.ns_t1 += (globaltimer_ns() - t1s) - (W.ns_t2 - t2_before);
+  (void)t0;
+  __syncwarp();
+  for (int i = lane; i < m; i += 32) map[cv[i]] = 0;
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
@@ -2215,6 +2479,8 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
   W.big_bits = pool.big_bits;
   W.nbig = pool.nbig;
   W.import_cap = pool.import_cap;
+  W.import_l = pool.import_l;
+  W.import_s = pool.import_s;
   W.slot_bits = pool.bits;
   W.nslot = pool.nslot;
   if (!kTiers)
@@ -2313,6 +2579,8 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
         W.gid = t.graph;
         W.gp = graph_at(W, t.graph);
         run_task(W, t);
+      } else if (t.v[1] == 1) {
+        tier1_from_slot(W, -2 - t.v[0]);  // an exported counts-tier child (sets the graph)
       } else {
         tier2_from_slot(W, -2 - t.v[0]);  // an exported bitmap sub-problem (sets the graph)
       }

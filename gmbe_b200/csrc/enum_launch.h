@@ -41,10 +41,6 @@ inline size_t enum_smem_bytes(const ScratchLayout& sl) {
 }
 // |P|*|L| from which a child is shared out while many warps wait for work.
 constexpr int32_t kShareMinWorkDefault = 256;
-// The same floor for a serving launch.  It stays at 64: the serving path was
-// exercised under load at 64, and the one loaded serving run at 256 stalled
-// without a found cause.
-constexpr int32_t kServeShareMinWorkDefault = 64;
 // P candidates per part of a root split into parts.
 constexpr int32_t kRangeChunkDefault = 64;
 // |P|*|C| above which a root of a two-tier launch (a graph whose worst roots

@@ -100,7 +100,7 @@ typedef struct mbe_params {
                            /*   still share out sub-problems.  <= 0 = never (default)      */
   int32_t share_min_work;  /* split_mode 0: while over an eighth of the warps wait for    */
                            /*   work, any child with |P|*|L| >= this is shared out, beyond */
-                           /*   the split test's children (0 = default: 256; 64 in a server) */
+                           /*   the split test's children (0 = default: 256)               */
   int32_t range_split_work; /* split_mode 0: a maximal root with |P|*|C| above this is   */
                            /*   split into parts of range_chunk P candidates; each part  */
                            /*   redoes the root's set-up and pushes, at the first level, */

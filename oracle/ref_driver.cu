@@ -14,7 +14,8 @@
 // (j = first .. first+count-1) is the roots v = j, j + stride, j + 2 stride,
 // ... below max_root (positions in the reference's own internal order after
 // -t/-o, from the lowest degree up; a max_root below 1 is that fraction of
-// all roots, 0 = every root).  The roots of a sample run on `threads`
+// all roots, 0 = every root).  `first` may instead be a comma-separated list
+// of sample offsets, run in that order (count is then ignored).  The roots of a sample run on `threads`
 // OpenMP threads, one finder object per thread (the finder's only mutable
 // state is its counter).  One line per sample:
 //   sample <j> roots <n> count <bicliques> seconds <wall time of the sample>
@@ -40,16 +41,17 @@
 #undef private
 #undef protected
 
-static int run_samples(CSRBiGraph* graph, int stride, int first, int count, int threads,
-                       double max_root_arg) {
-  if (stride < 1 || first < 0 || count < 1 || threads < 1) return 2;
+static int run_samples(CSRBiGraph* graph, int stride, const std::vector<int>& offsets,
+                       int threads, double max_root_arg) {
+  if (stride < 1 || offsets.empty() || threads < 1) return 2;
   long long max_root = max_root_arg > 0 && max_root_arg < 1
                            ? (long long)(max_root_arg * graph->V_size)
                            : (long long)max_root_arg;
   if (max_root <= 0 || max_root > graph->V_size) max_root = graph->V_size;
   std::vector<MbeaFinderBitset*> finders;
   for (int t = 0; t < threads; ++t) finders.push_back(new MbeaFinderBitset(graph));
-  for (int j = first; j < first + count; ++j) {
+  for (int j : offsets) {
+    if (j < 0) return 2;
     std::vector<int> roots;
     for (long long v = j % stride; v < max_root; v += stride) roots.push_back((int)v);
     for (auto* f : finders) f->maximal_nodes_ = 0;
@@ -95,8 +97,16 @@ int main(int argc, char** argv) {
     printf("read seconds %.3f V %d U %d E %d\n", get_cur_time() - t0, graph->V_size,
            graph->U_size, graph->edge_size);
     fflush(stdout);
-    rc = run_samples(graph, atoi(argv[5]), atoi(argv[6]), atoi(argv[7]), atoi(argv[8]),
-                     atof(argv[9]));
+    std::vector<int> offsets;
+    const std::string first = argv[6];
+    if (first.find(',') != std::string::npos) {
+      std::stringstream ss(first);
+      std::string item;
+      while (std::getline(ss, item, ',')) offsets.push_back(atoi(item.c_str()));
+    } else {
+      for (int j = atoi(argv[6]); j < atoi(argv[6]) + atoi(argv[7]); ++j) offsets.push_back(j);
+    }
+    rc = run_samples(graph, atoi(argv[5]), offsets, atoi(argv[8]), atof(argv[9]));
   } else {
     BicliqueFinder* finder = nullptr;
     if (sel == 0)
