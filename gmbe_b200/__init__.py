@@ -125,6 +125,8 @@ _sig = {
     "mbe_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(GraphInfo)]),
     "mbe_graph_free": (C.c_int, [C.c_void_p]),
     "mbe_enumerate": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]),
+    "mbe_enumerate_emit_stream": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result),
+                                            C.c_int64, C.c_void_p, C.c_void_p]),
     "mbe_enumerate_emit": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result), _P32,
                                      C.c_int64, C.POINTER(C.c_int64)]),
     "mbe_last_error_string": (C.c_char_p, []),
@@ -196,6 +198,10 @@ def make_opts(uvtrans=0, order=1, fast_mode=1, device=0) -> Opts:
     return Opts(uvtrans, order, fast_mode, device)
 
 
+_EMIT_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32), C.c_int32,
+                       C.c_void_p)
+
+
 class Graph:
     """A bipartite graph resident on the GPU (reference CSRBiGraph after
     Read + CopyToGpu).  V rows are .adj lines, entries U ids."""
@@ -259,6 +265,29 @@ class Graph:
             out.append((us, vs))
             pos += 2 + nu + nv
         return r, out
+
+    def enumerate_stream(self, on_biclique, ring_words: int = 1 << 22, **params) -> Result:
+        """mbe_enumerate_emit_stream: calls on_biclique(U ids, V ids) (tuples,
+        original ids) for every maximal biclique while the launch runs; a true
+        return value stops the calls.  Returns the Result."""
+        p = default_params(**params)
+        r = Result()
+        err = []
+
+        def cb(u, nu, v, nv, _user):
+            try:
+                return 1 if on_biclique(tuple(u[:nu]), tuple(v[:nv])) else 0
+            except Exception as e:  # noqa: BLE001 - surfaced after the call
+                err.append(e)
+                return 1
+
+        f = _EMIT_FN(cb)
+        rc = _lib.mbe_enumerate_emit_stream(self._h, C.byref(p), C.byref(r), int(ring_words),
+                                            C.cast(f, C.c_void_p), None)
+        if err:
+            raise err[0]
+        _check(rc)
+        return r
 
     def free(self):
         if self._h and self._h.value:

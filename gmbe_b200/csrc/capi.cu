@@ -8,6 +8,9 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <chrono>
+#include <functional>
+#include <thread>
 
 #include "engine.h"
 #include "tiers.h"
@@ -681,9 +684,13 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t rb, int32_t re, 
 }  // namespace
 
 // mbe_enumerate, optionally writing biclique records into d_emit (emit_cap
-// words) and reporting the words reserved in *emit_pos.
+// words) and reporting the words reserved in *emit_pos.  With d_emit_read
+// (ring mode) the records go to a ring the host drains: `drain` runs in this
+// thread, over and over, until the launch has finished.
 static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* out,
-                           int32_t* d_emit, long long emit_cap, unsigned long long* emit_pos) {
+                           int32_t* d_emit, long long emit_cap, unsigned long long* emit_pos,
+                           const unsigned long long* d_emit_read = nullptr,
+                           const std::function<void()>& drain = {}) {
   clear_error();
   if (!g || !out) return set_error(MBE_ERR_INVALID, "null argument");
   memset(out, 0, sizeof(*out));
@@ -740,6 +747,7 @@ static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* o
   if ((rc = engine_prepare(ws, spec, prm, &plan))) return rc;
   plan.ep.emit = d_emit;
   plan.ep.emit_cap = emit_cap;
+  plan.ep.emit_read = d_emit_read;
   if (plan.ep.n_big_warps > 0) {
     if (big_list.size() > ws.big_roots_cap) {
       cudaFree(ws.big_roots);
@@ -796,6 +804,16 @@ static int enumerate_graph(mbe_graph* g, const mbe_params* params, mbe_result* o
   CK(cudaMemcpyAsync(ws.d_prefix1, prefix, sizeof(prefix), cudaMemcpyHostToDevice, 0));
   if ((rc = engine_enqueue(ws, &plan, ws.d_graph1, ws.d_prefix1, ws.d_gres1, 1, 0, ws.ev0, ws.ev1)))
     return rc;
+  if (drain) {
+    // Producers may wait for room in the ring: drain it while the launch runs.
+    while (true) {
+      drain();
+      const cudaError_t q = cudaEventQuery(ws.ev1);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) return cuda_fail(q, "waiting for the launch");
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+  }
   EnumCtl ctl;
   unsigned long long gres[3];
   CK(cudaMemcpy(&ctl, ws.ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost));
@@ -829,76 +847,121 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   return enumerate_graph(g, params, out, nullptr, 0, nullptr);
 }
 
-int mbe_enumerate_emit(mbe_graph* g, const mbe_params* params, mbe_result* out, int32_t* buf,
-                       int64_t buf_words, int64_t* used_words) {
+namespace {
+
+// One record of the device ring -> the biclique in original ids and sides:
+// L (internal U ids) as given, R = N(L) from the internal U -> V lists.
+void decode_biclique(const HostGraph& h, std::vector<int32_t>& L, std::vector<int32_t>* us,
+                     std::vector<int32_t>* vs, std::vector<int32_t>& R, std::vector<int32_t>& tmp) {
+  int32_t best = L[0];
+  for (int32_t u : L)
+    if (h.rev_off[u + 1] - h.rev_off[u] < h.rev_off[best + 1] - h.rev_off[best]) best = u;
+  R.assign(h.rev_col.begin() + h.rev_off[best], h.rev_col.begin() + h.rev_off[best + 1]);
+  for (int32_t u : L) {
+    if (u == best) continue;
+    tmp.clear();
+    std::set_intersection(R.begin(), R.end(), h.rev_col.begin() + h.rev_off[u],
+                          h.rev_col.begin() + h.rev_off[u + 1], std::back_inserter(tmp));
+    R.swap(tmp);
+  }
+  us->clear();
+  vs->clear();
+  for (int32_t u : L) (h.swapped ? vs : us)->push_back(h.u_orig[u]);
+  for (int32_t v : R) (h.swapped ? us : vs)->push_back(h.v_orig[v]);
+  std::sort(us->begin(), us->end());
+  std::sort(vs->begin(), vs->end());
+}
+
+}  // namespace
+
+extern "C" int mbe_enumerate_emit_stream(mbe_graph* g, const mbe_params* params, mbe_result* out,
+                                         int64_t ring_words, mbe_emit_fn fn, void* user) {
+  clear_error();
+  if (!g || !out || !fn) return set_error(MBE_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(g->device));
+  int rc;
+  if ((rc = ensure_host_csr(g))) return rc;
+  // The ring holds at least one record of the largest L (a root's degree).
+  const long long cap = std::max<long long>({ring_words, (long long)g->capL + 2, 64});
+  int32_t* h_ring = nullptr;
+  unsigned long long* h_read = nullptr;
+  int32_t* d_ring = nullptr;
+  unsigned long long* d_read = nullptr;
+  cudaError_t e = cudaHostAlloc((void**)&h_ring, sizeof(int32_t) * (size_t)cap, cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&h_read, sizeof(unsigned long long), cudaHostAllocMapped);
+  if (e == cudaSuccess) {
+    memset(h_ring, 0, sizeof(int32_t) * (size_t)cap);
+    *h_read = 0;
+    e = cudaHostGetDevicePointer((void**)&d_ring, h_ring, 0);
+  }
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&d_read, h_read, 0);
+  if (e != cudaSuccess) {
+    if (h_ring) cudaFreeHost(h_ring);
+    if (h_read) cudaFreeHost(h_read);
+    return set_error(MBE_ERR_NOMEM, "emission ring of %lld words: %s", cap, cudaGetErrorString(e));
+  }
+  const HostGraph& h = g->h;
+  unsigned long long consumed = 0;
+  bool stopped = false;
+  std::vector<int32_t> L, R, tmp, us, vs;
+  auto drain = [&]() {
+    volatile int32_t* r = h_ring;
+    while (true) {
+      const int32_t len = r[consumed % (unsigned long long)cap];
+      if (len <= 0) return;
+      L.resize((size_t)len);
+      for (int32_t i = 0; i < len; ++i) L[i] = r[(consumed + 2 + i) % (unsigned long long)cap];
+      for (int32_t i = 0; i < len + 2; ++i) r[(consumed + i) % (unsigned long long)cap] = 0;
+      consumed += (unsigned long long)len + 2;
+      *(volatile unsigned long long*)h_read = consumed;
+      if (!stopped) {
+        decode_biclique(h, L, &us, &vs, R, tmp);
+        if (fn(us.data(), (int32_t)us.size(), vs.data(), (int32_t)vs.size(), user) != 0)
+          stopped = true;
+      }
+    }
+  };
+  unsigned long long reserved = 0;
+  rc = enumerate_graph(g, params, out, d_ring, cap, &reserved, d_read, drain);
+  if (rc == MBE_OK) {
+    // Every reserved record is committed once the launch has ended.
+    while (consumed < reserved) drain();
+  }
+  cudaFreeHost(h_ring);
+  cudaFreeHost(h_read);
+  return rc;
+}
+
+extern "C" int mbe_enumerate_emit(mbe_graph* g, const mbe_params* params, mbe_result* out,
+                                  int32_t* buf, int64_t buf_words, int64_t* used_words) {
   clear_error();
   if (!g || !out || !used_words || buf_words < 0 || (buf_words > 0 && !buf))
     return set_error(MBE_ERR_INVALID, "null or negative argument");
   *used_words = 0;
-  CK(cudaSetDevice(g->device));
-  // Device records ([|L|, graph, L]) are never longer than the output records
-  // ([|U|, |V|, U, V]) they become, so a device buffer of buf_words suffices.
-  const long long dcap = std::max<long long>(buf_words, 2);
-  int32_t* d_emit = nullptr;
-  CK(cudaMalloc((void**)&d_emit, sizeof(int32_t) * (size_t)dcap));
-  int rc = MBE_OK;
-  unsigned long long reserved = 0;
-  std::vector<int32_t> dev;
-  cudaError_t e = cudaMemset(d_emit, 0, sizeof(int32_t) * (size_t)dcap);
-  if (e != cudaSuccess) rc = set_error(MBE_ERR_CUDA, "clearing the record buffer: %s", cudaGetErrorString(e));
-  if (!rc) rc = enumerate_graph(g, params, out, d_emit, dcap, &reserved);
-  if (!rc) {
-    dev.resize((size_t)std::min<unsigned long long>(reserved, (unsigned long long)dcap));
-    e = cudaMemcpy(dev.data(), d_emit, sizeof(int32_t) * dev.size(), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) rc = set_error(MBE_ERR_CUDA, "reading the records: %s", cudaGetErrorString(e));
-  }
-  cudaFree(d_emit);
+  struct Sink {
+    int32_t* buf;
+    int64_t cap, used;
+    bool full;
+  } sink{buf, buf_words, 0, false};
+  auto put = [](const int32_t* u, int32_t nu, const int32_t* v, int32_t nv, void* p) -> int {
+    Sink* s = static_cast<Sink*>(p);
+    const int64_t need = 2 + (int64_t)nu + nv;
+    if (s->used + need > s->cap) {
+      s->full = true;
+      return 1;  // stop delivering; the enumeration still completes
+    }
+    s->buf[s->used] = nu;
+    s->buf[s->used + 1] = nv;
+    std::copy(u, u + nu, s->buf + s->used + 2);
+    std::copy(v, v + nv, s->buf + s->used + 2 + nu);
+    s->used += need;
+    return 0;
+  };
+  int rc = mbe_enumerate_emit_stream(g, params, out, int64_t(1) << 22, put, &sink);
+  *used_words = sink.used;
   if (rc) return rc;
-  // Records: R = N(L) from the internal U -> V lists; both sides to original
-  // ids (internal U is the original V side when -t swapped them).
-  if ((rc = ensure_host_csr(g))) return rc;
-  const HostGraph& h = g->h;
-  std::vector<int32_t> L, R, tmp, us, vs;
-  size_t pos = 0;
-  int64_t used = 0;
-  bool full = false;
-  while (pos + 2 <= dev.size() && dev[pos] > 0) {
-    const int32_t nl = dev[pos];
-    if (pos + 2 + (size_t)nl > dev.size()) break;
-    L.assign(dev.begin() + pos + 2, dev.begin() + pos + 2 + nl);
-    pos += 2 + (size_t)nl;
-    int32_t best = L[0];
-    for (int32_t u : L)
-      if (h.rev_off[u + 1] - h.rev_off[u] < h.rev_off[best + 1] - h.rev_off[best]) best = u;
-    R.assign(h.rev_col.begin() + h.rev_off[best], h.rev_col.begin() + h.rev_off[best + 1]);
-    for (int32_t u : L) {
-      if (u == best) continue;
-      tmp.clear();
-      std::set_intersection(R.begin(), R.end(), h.rev_col.begin() + h.rev_off[u],
-                            h.rev_col.begin() + h.rev_off[u + 1], std::back_inserter(tmp));
-      R.swap(tmp);
-    }
-    us.clear();
-    vs.clear();
-    for (int32_t u : L) (h.swapped ? vs : us).push_back(h.u_orig[u]);
-    for (int32_t v : R) (h.swapped ? us : vs).push_back(h.v_orig[v]);
-    std::sort(us.begin(), us.end());
-    std::sort(vs.begin(), vs.end());
-    const int64_t need = 2 + (int64_t)us.size() + (int64_t)vs.size();
-    if (used + need > buf_words) {
-      full = true;
-      break;
-    }
-    buf[used] = (int32_t)us.size();
-    buf[used + 1] = (int32_t)vs.size();
-    std::copy(us.begin(), us.end(), buf + used + 2);
-    std::copy(vs.begin(), vs.end(), buf + used + 2 + us.size());
-    used += need;
-  }
-  *used_words = used;
-  if (full || reserved > (unsigned long long)dcap)
-    return set_error(MBE_ERR_CAPACITY, "record buffer of %lld words too small (%llu device words reserved)",
-                     (long long)buf_words, reserved);
+  if (sink.full)
+    return set_error(MBE_ERR_CAPACITY, "record buffer of %lld words too small", (long long)buf_words);
   return MBE_OK;
 }
 

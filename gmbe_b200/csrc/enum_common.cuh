@@ -181,6 +181,7 @@ struct EnumParams {
   int32_t eager_share;        // 1: counts-tier children passing the split test always go
   int32_t* emit;              // biclique records [|L|, graph, L ids...], or null
   long long emit_cap;         // words in emit
+  const unsigned long long* emit_read;  // ring mode: words the host has consumed (else null)
   int32_t server;             // 1: graphs arrive while the launch runs (ServeLink)
   ServeLink serve;
   // Two scratch tiers (single-graph launches only).  Warps [0, n_big_warps)

@@ -185,69 +185,114 @@ __device__ int collect_bits(uint32_t* bits, int words, int32_t* out, int cap) {
 }
 
 // Emission (opt-in): appends a maximal biclique's L to the launch's record
-// buffer as [|L|, graph, internal U ids of L...]; R is N(L).  A record that
-// does not fit entirely is dropped (the reserved word count keeps growing past
-// the buffer, which tells the host).  The host zeroes the buffer first, so a
-// zero length word marks the end of what was written.  Kept out of line and
-// given plain arguments: inlined at its four call sites, the code grew the
+// buffer as [|L|, graph, internal U ids of L...]; R is N(L).  Two forms:
+//  - a buffer (rd null): a record that does not fit entirely is dropped (the
+//    reserved word count keeps growing past the buffer, which tells the
+//    host); the host zeroes the buffer first and reads it after the launch;
+//  - a ring in host-mapped memory (rd = the host's consumed word count):
+//    positions grow without bound and index the ring modulo its size; a
+//    producer whose record would overrun words the host has not consumed
+//    waits for it (bounded by wait_ns: past it the launch fails with a
+//    timeout status and the record is dropped).  The host drains the ring
+//    while the launch runs and zeroes what it consumed.
+// In both, the body and graph words are made visible system-wide before the
+// length word, which commits the record (the host waits for a non-zero
+// length at the next position).  Kept out of line and given plain
+// arguments: inlined at its four call sites, the code grew the
 // enumeration's hot loops enough to slow every launch by a quarter.
-// Reserves a record of `count` ids; -1 if it does not fit.
-__device__ __forceinline__ long long emit_reserve(EnumCtl* ctl, long long cap, int count) {
-  unsigned long long pos = 0;
-  if (lane_id() == 0) pos = atomicAdd(&ctl->emit_pos, (unsigned long long)count + 2);
-  pos = __shfl_sync(kFull, pos, 0);
-  return pos + (unsigned long long)count + 2 > (unsigned long long)cap ? -1LL : (long long)pos;
+struct EmitDst {
+  int32_t* buf;
+  long long cap;                        // words
+  const unsigned long long* rd;         // ring: words the host has consumed
+  long long wait_ns;                    // ring: longest wait for room
+};
+
+__device__ __forceinline__ EmitDst emit_dst(const EnumParams& p) {
+  return EmitDst{p.emit, p.emit_cap, p.emit_read, p.idle_ns_limit};
 }
 
-__device__ __forceinline__ void emit_header(int32_t* buf, long long pos, int count, int gid) {
+// Reserves a record of `count` ids (lane-uniform); -1 if it is dropped.
+__device__ long long emit_reserve(EnumCtl* ctl, const EmitDst& d, int count) {
+  const unsigned long long need = (unsigned long long)count + 2;
+  long long pos = 0;
   if (lane_id() == 0) {
-    buf[pos + 1] = gid;
-    buf[pos] = count;
+    const unsigned long long at = atomicAdd(&ctl->emit_pos, need);
+    if (!d.rd) {
+      pos = at + need > (unsigned long long)d.cap ? -1LL : (long long)at;
+    } else if (need > (unsigned long long)d.cap) {
+      pos = -1;
+      set_status(ctl, kStCapacity, ((unsigned long long)6 << 32) | (unsigned)count);
+    } else {
+      pos = (long long)at;
+      const uint64_t t0 = globaltimer_ns();
+      while (at + need > *(volatile const unsigned long long*)d.rd + (unsigned long long)d.cap) {
+        if (*(volatile int32_t*)&ctl->abort || globaltimer_ns() - t0 > (uint64_t)d.wait_ns) {
+          set_status(ctl, kStTimeout, at);
+          pos = -1;
+          break;
+        }
+        __nanosleep(1000);
+      }
+    }
+  }
+  return __shfl_sync(kFull, pos, 0);
+}
+
+__device__ __forceinline__ int32_t& emit_at(const EmitDst& d, long long pos) {
+  return d.buf[(unsigned long long)pos % (unsigned long long)d.cap];
+}
+
+__device__ __forceinline__ void emit_header(const EmitDst& d, long long pos, int count, int gid) {
+  __threadfence_system();
+  __syncwarp();
+  if (lane_id() == 0) {
+    emit_at(d, pos + 1) = gid;
+    __threadfence_system();
+    emit_at(d, pos) = count;
   }
   __syncwarp();
 }
 
 // L = ids[idx[i]] (or ids[i] when idx is null) for i < n.
-__device__ __noinline__ void emit_list(EnumCtl* ctl, int32_t* buf, long long cap, int gid, int n,
+__device__ __noinline__ void emit_list(EnumCtl* ctl, EmitDst d, int gid, int n,
                                        const int32_t* ids, const int32_t* idx) {
-  const long long pos = emit_reserve(ctl, cap, n);
+  const long long pos = emit_reserve(ctl, d, n);
   if (pos < 0) return;
-  for (int i = (int)lane_id(); i < n; i += 32) buf[pos + 2 + i] = idx ? ids[idx[i]] : ids[i];
-  emit_header(buf, pos, n, gid);
+  for (int i = (int)lane_id(); i < n; i += 32) emit_at(d, pos + 2 + i) = idx ? ids[idx[i]] : ids[i];
+  emit_header(d, pos, n, gid);
 }
 
 // L = ids[l] for the l < nscan with llevel[l] == level, count of them.
-__device__ __noinline__ void emit_level(EnumCtl* ctl, int32_t* buf, long long cap, int gid,
-                                        int count, int nscan, const int32_t* llevel, int level,
-                                        const int32_t* ids) {
-  const long long pos = emit_reserve(ctl, cap, count);
+__device__ __noinline__ void emit_level(EnumCtl* ctl, EmitDst d, int gid, int count, int nscan,
+                                        const int32_t* llevel, int level, const int32_t* ids) {
+  const long long pos = emit_reserve(ctl, d, count);
   if (pos < 0) return;
   int out = 0;
   for (int b0 = 0; b0 < nscan; b0 += 32) {
     const int l = b0 + (int)lane_id();
     const bool s = l < nscan && llevel[l] == level;
     const unsigned bal = __ballot_sync(kFull, s);
-    if (s) buf[pos + 2 + out + __popc(bal & lanemask_lt())] = ids[l];
+    if (s) emit_at(d, pos + 2 + out + __popc(bal & lanemask_lt())) = ids[l];
     out += __popc(bal);
   }
-  emit_header(buf, pos, count, gid);
+  emit_header(d, pos, count, gid);
 }
 
 // L = lid[b] for the set bits b of the K-word mask (m0..m3), count of them.
-__device__ __noinline__ void emit_mask(EnumCtl* ctl, int32_t* buf, long long cap, int gid,
-                                       int count, int K, uint32_t m0, uint32_t m1, uint32_t m2,
-                                       uint32_t m3, const int32_t* lid) {
-  const long long pos = emit_reserve(ctl, cap, count);
+__device__ __noinline__ void emit_mask(EnumCtl* ctl, EmitDst d, int gid, int count, int K,
+                                       uint32_t m0, uint32_t m1, uint32_t m2, uint32_t m3,
+                                       const int32_t* lid) {
+  const long long pos = emit_reserve(ctl, d, count);
   if (pos < 0) return;
   const int lane = (int)lane_id();
   int out = 0;
   for (int w = 0; w < K; ++w) {
     const uint32_t m = w == 0 ? m0 : (w == 1 ? m1 : (w == 2 ? m2 : m3));
     const bool s = (m >> lane) & 1u;
-    if (s) buf[pos + 2 + out + __popc(m & lanemask_lt())] = lid[w * 32 + lane];
+    if (s) emit_at(d, pos + 2 + out + __popc(m & lanemask_lt())) = lid[w * 32 + lane];
     out += __popc(m);
   }
-  emit_header(buf, pos, count, gid);
+  emit_header(d, pos, count, gid);
 }
 
 // Serving block of graph `gid` (a block index into the arena, which the
@@ -639,7 +684,7 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
         W.cnt += 1;
         W.hash += biclique_hash(*W.gp, sL, (uint64_t)kn, sR, nR);
         if (emitting)
-          emit_mask(W.ctl, W.p.emit, W.p.emit_cap, W.gid, kn, K, Ln[0], K > 1 ? Ln[1 % K] : 0u,
+          emit_mask(W.ctl, emit_dst(W.p), W.gid, kn, K, Ln[0], K > 1 ? Ln[1 % K] : 0u,
                     K > 2 ? Ln[2 % K] : 0u, K > 3 ? Ln[3 % K] : 0u, src.lid);
       } else {
         W.nonmax += 1;
@@ -1169,7 +1214,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   if (ism) {
     W.cnt += 1;
     W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
-    if (W.p.emit) emit_list(W.ctl, W.p.emit, W.p.emit_cap, W.gid, n, t.L, lp);
+    if (W.p.emit) emit_list(W.ctl, emit_dst(W.p), W.gid, n, t.L, lp);
   } else {
     W.nonmax += 1;
   }
@@ -1524,7 +1569,7 @@ __device__ void tier1_run(Warp& W, const T1& t) {
         W.cnt += 1;
         W.hash += biclique_hash(*W.gp, sL, (uint64_t)kept, sR, nR);
         if (emitting)
-          emit_level(W.ctl, W.p.emit, W.p.emit_cap, W.gid, kept, t.nL, llevel, level, t.L);
+          emit_level(W.ctl, emit_dst(W.p), W.gid, kept, t.nL, llevel, level, t.L);
       } else {
         W.nonmax += 1;
       }
@@ -2247,7 +2292,7 @@ __device__ void run_task(Warp& W, const Task& t) {
     sL = warp_sum(sL);
     W.cnt += 1;
     W.hash += biclique_hash(g, sL, (uint64_t)nL, sR, nR);
-    if (W.p.emit) emit_list(W.ctl, W.p.emit, W.p.emit_cap, W.gid, nL, L, nullptr);
+    if (W.p.emit) emit_list(W.ctl, emit_dst(W.p), W.gid, nL, L, nullptr);
   }
   bool done = nL <= 1 || np == 0;
   // ---- split (src/IterFinderGpu.cu:835-858) ----

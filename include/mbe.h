@@ -215,11 +215,31 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out);
  * counterpart in the reference, which only counts): records
  * [|U|, |V|, U ids ascending, V ids ascending] in original ids and sides,
  * packed one after another, *used_words in all.  The kernel emits each
- * biclique's L side into a device buffer as it is found; the host derives the
- * other side as the common neighbourhood of L.  MBE_ERR_CAPACITY (with the
- * records that fit, *used_words of them) when buf is too small. */
+ * biclique's L side into a ring the host drains while the launch runs (see
+ * mbe_enumerate_emit_stream); the host derives the other side as the common
+ * neighbourhood of L.  MBE_ERR_CAPACITY (with the records that fit,
+ * *used_words of them) when buf is too small; count and hash stay exact. */
 int mbe_enumerate_emit(mbe_graph* g, const mbe_params* params, mbe_result* out, int32_t* buf,
                        int64_t buf_words, int64_t* used_words);
+
+/* One maximal biclique, in original ids and sides, ids ascending; return 0 to
+ * go on, non-zero to receive no more (the enumeration still completes and
+ * `out` stays exact). */
+typedef int (*mbe_emit_fn)(const int32_t* u_ids, int32_t n_u, const int32_t* v_ids, int32_t n_v,
+                           void* user);
+
+/* As mbe_enumerate, handing every maximal biclique to `fn` while the launch
+ * runs (no counterpart in the reference, whose GPU path only counts; its CPU
+ * finders print each biclique at the count site, src/BicliqueFinder.cu:20-57).
+ * The kernel writes each biclique's L side into a ring of ring_words int32
+ * words in pinned, device-mapped host memory (at least one largest record);
+ * this call drains and decodes the ring in the calling thread while the
+ * kernel runs, and a producer that would overrun undrained records waits
+ * for room.  Any number of bicliques passes through a ring of fixed size.
+ * mbe_enumerate_emit is this call with a 2^22-word ring and a callback that
+ * fills the caller's buffer. */
+int mbe_enumerate_emit_stream(mbe_graph* g, const mbe_params* params, mbe_result* out,
+                              int64_t ring_words, mbe_emit_fn fn, void* user);
 
 /* Thread-local message of the last failed call ("" if none). */
 const char* mbe_last_error_string(void);

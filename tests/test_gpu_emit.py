@@ -106,3 +106,47 @@ def test_emit_buffer_too_small(gm):
         with pytest.raises(gm.MBEError) as ei:
             G.enumerate_emit(buf_words=64)
         assert ei.value.name == "MBE_ERR_CAPACITY"
+
+
+@pytest.mark.last
+@pytest.mark.parametrize("ring_words", [64, 1000, 1 << 16])
+def test_stream_through_a_ring_smaller_than_the_output(gm, ring_words):
+    # The kernel writes into a ring the host drains while the launch runs;
+    # with 64 words the ring holds a handful of records at a time, so the
+    # producers wait on the host again and again.  Every biclique arrives
+    # once, and the set equals the buffered emission's and the oracle's.
+    ro, co, nU = planted(300, 200, blocks=6, seed=3, bsize=14)
+    want = oracle.gmbe(ro, co, nU)
+    with gm.Graph.from_csr(ro, co, nU, uvtrans=1) as G:
+        got = []
+        r = G.enumerate_stream(lambda u, v: got.append((u, v)), ring_words=ring_words)
+        rb, buffered = G.enumerate_emit(buf_words=1 << 24)
+    assert (r.count, r.set_hash) == (want.count, want.set_hash)
+    assert len(got) == len(set(got)) == want.count
+    assert set(got) == set(buffered)
+    assert set_hash(got) == want.set_hash
+    assert sum(2 + len(u) + len(v) for u, v in got) > 4 * ring_words
+
+
+@pytest.mark.last
+def test_stream_stops_delivering_but_counts_exactly(gm):
+    ro, co, nU = hub_graph(2)
+    want = oracle.gmbe(ro, co, nU)
+    with gm.Graph.from_csr(ro, co, nU, uvtrans=1) as G:
+        got = []
+        r = G.enumerate_stream(lambda u, v: got.append((u, v)) or len(got) >= 10, ring_words=256)
+    assert len(got) == 10
+    assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+@pytest.mark.last
+def test_stream_with_two_tiers_and_exported_children(gm):
+    # Records written by warps running exported children and big-root parts.
+    ro, co, nU = planted(300, 200, blocks=6, seed=3, bsize=14)
+    want = oracle.gmbe(ro, co, nU)
+    with gm.Graph.from_csr(ro, co, nU, uvtrans=1) as G:
+        got = []
+        r = G.enumerate_stream(lambda u, v: got.append((u, v)), ring_words=512, big_two_hop=64,
+                               range_split_work=1, range_chunk=2, share_min_work=1)
+    assert (r.count, r.set_hash) == (want.count, want.set_hash)
+    assert len(got) == len(set(got)) == want.count and set_hash(got) == want.set_hash
