@@ -581,8 +581,7 @@ def main():
         kern_mean = kern_total / args.steps
         alg_step = alg_all / args.steps / world
         ach = alg_step / (kern_mean / 1e3) / 1e9
-        consts = load_consts("large")
-        tpb = consts.get("traffic_bytes_per_biclique")
+        tpb = (load_json(CONSTS) or {}).get(WORKLOAD, {}).get("traffic_bytes_per_biclique")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

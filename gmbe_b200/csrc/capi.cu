@@ -392,17 +392,18 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.root_split = prm.split_mode == 1 ? 0 : std::max(prm.root_split_size, 0);
   ep.share_min_work = prm.share_min_work > 0 ? prm.share_min_work : kShareMinWorkDefault;
   apply_range_split(prm, &ep.range_work, &ep.range_chunk);
+  // Heavy roots are split into parts by default: single roots with |P|*|C|
+  // above 10^9 (graphs of hundreds of thousands of candidates per root)
+  // otherwise run for most of a launch on one warp.
+  if (prm.range_split_work == 0 && prm.split_mode != 1) ep.range_work = kRangeWorkDefault;
   ep.eager_share = eager_share_of(prm);
   ep.n_graphs = spec.n_graphs;
   ep.n_big_warps = n_big;
   ep.big_sl = big_sl;
   if (n_big > 0) {
-    // Vertex-tuple children could need the big tier: off.  Heavy roots are
-    // split into parts by default (a big root's parts run on big warps only):
-    // in graphs whose worst roots do not fit every warp, single roots
-    // otherwise run for most of a launch on one warp.
+    // Vertex-tuple children could need the big tier: off.  Root parts stay
+    // on (a big root's parts run on big warps only).
     ep.root_split = 0;
-    if (prm.range_split_work == 0 && prm.split_mode != 1) ep.range_work = kRangeWorkTiersDefault;
   }
   plan->pool.slots = ws.slots;
   plan->pool.bits = ws.slot_bits;

@@ -43,9 +43,9 @@ inline size_t enum_smem_bytes(const ScratchLayout& sl) {
 constexpr int32_t kShareMinWorkDefault = 256;
 // P candidates per part of a root split into parts.
 constexpr int32_t kRangeChunkDefault = 64;
-// |P|*|C| above which a root of a two-tier launch (a graph whose worst roots
-// do not fit every warp) is split into parts unless the caller says otherwise.
-constexpr int32_t kRangeWorkTiersDefault = 1000000000;
+// |P|*|C| above which a root is split into parts unless the caller says
+// otherwise (no root of the medium or batched workloads comes near it).
+constexpr int32_t kRangeWorkDefault = 1000000000;
 
 
 // Per-warp scratch layout for the given capacities.

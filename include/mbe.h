@@ -105,9 +105,9 @@ typedef struct mbe_params {
                            /*   split into parts of range_chunk P candidates; each part  */
                            /*   redoes the root's set-up and pushes, at the first level, */
                            /*   only the candidates whose id hashes to it (earlier parts */
-                           /*   act as Q).  0 = default: never, except in a launch with */
-                           /*   two scratch tiers, where it is 10^9 and a listed big     */
-                           /*   root's parts run on the big warps only; < 0 = never      */
+                           /*   act as Q).  0 = default, 10^9; < 0 = never.  In a       */
+                           /*   launch with two scratch tiers a listed big root's parts  */
+                           /*   run on the big warps only                                */
   int32_t range_chunk;     /* P candidates per part (0 = default 64)                     */
   int32_t eager_share;     /* split_mode 0: a child of the counts tier (|L| > bitmap_max_l) */
                            /*   that passes the split test is shared out even while no  */
