@@ -109,7 +109,7 @@ def test_emit_buffer_too_small(gm):
 
 
 @pytest.mark.last
-@pytest.mark.parametrize("ring_words", [64, 1000, 1 << 16])
+@pytest.mark.parametrize("ring_words", [64, 1000, 4096])
 def test_stream_through_a_ring_smaller_than_the_output(gm, ring_words):
     # The kernel writes into a ring the host drains while the launch runs;
     # with 64 words the ring holds a handful of records at a time, so the
