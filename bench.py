@@ -616,6 +616,9 @@ def main():
                 except Exception as e:  # noqa: BLE001
                     log(f"{name} leg failed: {e}")
                     line[name] = {"error": f"{type(e).__name__}: {e}"}
+            # The serving leg's own process needs the memory this one caches.
+            gm.release_device(local)
+            torch.cuda.empty_cache()
             line["serving"] = serving_leg_isolated()
         if world == 1 and not args.no_cpu_baseline:
             log("CPU baseline")

@@ -63,7 +63,8 @@ class Params(C.Structure):
                 ("eager_share", C.c_int32), ("big_two_hop", C.c_int32),
                 ("big_warps", C.c_int32), ("l2_window", C.c_int32),
                 ("time_limit_ns", C.c_int64), ("touch_scan", C.c_int32),
-                ("slot_records", C.c_int32)]
+                ("slot_records", C.c_int32),
+                ("share_counts", C.c_int32), ("reserved_r", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -124,6 +125,7 @@ _sig = {
                                             C.POINTER(Opts), C.POINTER(C.c_void_p)]),
     "mbe_graph_get_info": (C.c_int, [C.c_void_p, C.POINTER(GraphInfo)]),
     "mbe_graph_free": (C.c_int, [C.c_void_p]),
+    "mbe_device_release": (C.c_int, [C.c_int32]),
     "mbe_enumerate": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]),
     "mbe_enumerate_emit_stream": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Result),
                                             C.c_int64, C.c_void_p, C.c_void_p]),
@@ -182,6 +184,11 @@ def _i32(a) -> np.ndarray:
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_P32)
+
+
+def release_device(device: int = 0):
+    """mbe_device_release: hands back the device memory cached between calls."""
+    _check(_lib.mbe_device_release(int(device)))
 
 
 def default_params(**kw) -> Params:

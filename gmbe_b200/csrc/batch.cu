@@ -105,7 +105,8 @@ bool same_global(const mbe_params& a, const mbe_params& c) {
          a.root_split_size == c.root_split_size && a.share_min_work == c.share_min_work &&
          a.range_split_work == c.range_split_work && a.range_chunk == c.range_chunk &&
          a.eager_share == c.eager_share && a.time_limit_ns == c.time_limit_ns &&
-         a.touch_scan == c.touch_scan && a.slot_records == c.slot_records;
+         a.touch_scan == c.touch_scan && a.slot_records == c.slot_records &&
+         a.share_counts == c.share_counts && a.l2_window == c.l2_window;
 }
 
 // Captures (or re-captures) the launch when the workspace or the global

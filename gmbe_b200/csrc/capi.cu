@@ -386,6 +386,7 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
   ep.time_limit_ns = std::max<int64_t>(prm.time_limit_ns, 0);
   ep.touch_scan = prm.touch_scan > 0 ? 1 : (prm.touch_scan < 0 ? -1 : 0);
   ep.slot_records = std::max(prm.slot_records, 0);
+  ep.share_counts = prm.share_counts < 0 ? 0 : 1;
   ep.record_exit = prm.sm_timing ? 1 : 0;
   ep.vertex_split = prm.split_mode == 1 ? 1 : 0;
   // Heavy roots split into vertex tuples (sub-problem sharing mode only).
@@ -604,6 +605,45 @@ int mbe_graph_get_info(const mbe_graph* g, mbe_graph_info* info) {
   info->U_2degree = g->h.U_2degree;
   info->V_2degree = g->h.V_2degree;
   info->swapped = g->h.swapped;
+  return MBE_OK;
+}
+
+int mbe_device_release(int32_t device) {
+  clear_error();
+  if (device < 0 || device >= kMaxDevices) return set_error(MBE_ERR_INVALID, "bad device");
+  Workspace& ws = g_ws[device];
+  std::lock_guard<std::mutex> lock(ws.mu);
+  CK(cudaSetDevice(device));
+  CK(cudaDeviceSynchronize());
+  for (void* p : {(void*)ws.scratch, (void*)ws.ctl, (void*)ws.q_tasks, (void*)ws.q_seq,
+                  (void*)ws.exit_ns, (void*)ws.slots, (void*)ws.slot_bits, (void*)ws.big_slots,
+                  (void*)ws.big_slot_bits, (void*)ws.d_graph1, (void*)ws.d_prefix1,
+                  (void*)ws.d_gres1, (void*)ws.big_roots, (void*)ws.big_flag, (void*)ws.big_parts})
+    cudaFree(p);
+  ws.scratch = nullptr;
+  ws.scratch_bytes = 0;
+  ws.ctl = nullptr;
+  ws.q_tasks = nullptr;
+  ws.q_seq = nullptr;
+  ws.q_cap = 0;
+  ws.exit_ns = nullptr;
+  ws.exit_cap = 0;
+  ws.slots = nullptr;
+  ws.slot_bits = nullptr;
+  ws.nslot = 0;
+  ws.big_slots = nullptr;
+  ws.big_slot_bits = nullptr;
+  ws.nbig_slot = 0;
+  ws.d_graph1 = nullptr;
+  ws.d_prefix1 = nullptr;
+  ws.d_gres1 = nullptr;
+  ws.big_roots = nullptr;
+  ws.big_flag = nullptr;
+  ws.big_parts = nullptr;
+  ws.big_roots_cap = ws.big_flag_cap = ws.big_parts_cap = 0;
+  ws.map_pitch_words = ws.map_words = -1;
+  ws.map_warps = -1;
+  ++ws.gen;  // captured batch launches refer to the old buffers
   return MBE_OK;
 }
 

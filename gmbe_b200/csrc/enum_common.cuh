@@ -171,6 +171,8 @@ struct EnumParams {
   int64_t time_limit_ns;      // > 0: the launch gives up after this long (kStDeadline)
   int32_t touch_scan;         // 0 auto, 1 always scan the global touch bitmap, -1 never
   int32_t slot_records;       // > 0: regular slots take children of at most this many records
+  int32_t share_counts;       // 1: counts-tier children may go to idle warps as vertex lists
+  int32_t pad_sc;
   int32_t record_exit;        // -p
   int32_t vertex_split;       // 1: GMBE vertex-tuple child tasks at task set-up
   int32_t n_graphs;           // graphs of this launch (1 for a single enumeration)

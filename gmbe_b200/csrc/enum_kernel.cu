@@ -1363,7 +1363,7 @@ constexpr int kFrameHdr = 16;
 // Whether a counts-tier child of `kept` rows (`kent` entries) may be shared
 // out now: slots exist, every warp has room for it, warps wait for work.
 __device__ __forceinline__ bool t1_export_wanted(Warp& W, int kept, long long kent) {
-  if (W.nslot == 0 && W.nbig == 0) return false;
+  if (!W.p.share_counts || (W.nslot == 0 && W.nbig == 0)) return false;
   if (kept > W.import_l || kent > (long long)W.import_s) return false;
   return export_demand(W) != 0;
 }

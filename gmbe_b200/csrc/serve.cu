@@ -194,6 +194,7 @@ int allocate(mbe_server* s) {
   ep.idle_ns_limit = 600LL * 1000000000LL;
   ep.vertex_split = s->prm.split_mode == 1 ? 1 : 0;
   ep.root_split = s->prm.split_mode == 1 ? 0 : std::max(s->prm.root_split_size, 0);
+  ep.share_counts = s->prm.share_counts < 0 ? 0 : 1;
   ep.share_min_work =
       s->prm.share_min_work > 0 ? s->prm.share_min_work : kShareMinWorkDefault;
   apply_range_split(s->prm, &ep.range_work, &ep.range_chunk);

@@ -137,6 +137,9 @@ typedef struct mbe_params {
   int32_t slot_records;    /* a shared-out child with more candidates than this (0 =     */
                            /*   as many as a 128 KiB slot holds) goes through a 4 MiB     */
                            /*   slot instead; results do not depend on it                 */
+  int32_t share_counts;    /* counts-tier children (|L| above the bitmap tier) go to      */
+                           /*   idle warps as vertex lists: 0 = default, yes; < 0 = no     */
+  int32_t reserved_r;      /* zero */
 } mbe_params;
 
 typedef struct mbe_result {
@@ -204,6 +207,14 @@ int mbe_graph_get_info(const mbe_graph* g, mbe_graph_info* info);
 
 /* Release host and device memory.  Replaces CSRBiGraph::Reset (src/BiGraph.cu:433-454). */
 int mbe_graph_free(mbe_graph* g);
+
+/* Release the device memory the library keeps on `device` between calls of
+ * mbe_enumerate and of batches (per-warp scratch, split ring, export slots;
+ * on the largest graphs most of the device).  The next call allocates again.
+ * The reference allocates and frees per finder object
+ * (src/IterFinderGpu.cu:1056-1093); this engine caches, and this call is how
+ * a caller hands the memory back, e.g. before another process uses the GPU. */
+int mbe_device_release(int32_t device);
 
 /* ---- enumeration --------------------------------------------------------- */
 /* Count all maximal bicliques of g and their set hash on g's device.

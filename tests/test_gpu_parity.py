@@ -248,3 +248,17 @@ def test_large_export_slots(gm, slot_records, case):
         r = run(gm, ro, co, nU, slot_records=slot_records, share_min_work=1, **params)
         assert r.status == 0
         assert (r.count, r.set_hash) == (want.count, want.set_hash), params
+
+
+def test_share_counts_switch_and_device_release(gm):
+    # Counts-tier children shared out or kept (results equal), and the
+    # device's cached workspace handed back between calls.
+    ro, co, nU = hub_graph(4)
+    want = oracle.gmbe(ro, co, nU)
+    with gm.Graph.from_csr(ro, co, nU, uvtrans=1) as G:
+        for sc in (0, -1, 0):
+            r = G.enumerate(share_counts=sc, share_min_work=1)
+            assert (r.count, r.set_hash) == (want.count, want.set_hash)
+            gm.release_device(0)
+        r = G.enumerate()
+        assert (r.count, r.set_hash) == (want.count, want.set_hash)
