@@ -260,6 +260,25 @@ def run_profile_case():
 BATCH_ORACLE = os.path.join(ROOT, "tests", "golden", "batch_oracle.json")
 
 
+def run_profile_batch(n=512):
+    """A reduced batched launch for ncu captures: the first n graphs of the
+    batched workload (seeds 1000..1000+n-1) in one launch, captured and
+    replayed twice, every per-graph count and set hash checked against the
+    oracle's (tests/golden/batch_oracle.json)."""
+    import gmbe_b200 as gm
+    orc = load_json(BATCH_ORACLE)
+    want = list(zip(orc["count"], (int(h, 16) for h in orc["set_hash"])))[:n]
+    B = gm.Batch([gm.batch_graph(1000 + i) for i in range(n)])
+    runs = [B.run() for _ in range(2)]
+    B.free()
+    for per, _ in runs:
+        if [(r.count, r.set_hash) for r in per] != want:
+            raise SystemExit("batch profile case: results differ from the oracle's")
+    tot = runs[-1][1]
+    print(json.dumps({"profile_case": f"batched, graphs 0..{n - 1}", "bicliques": tot.count,
+                      "kernel_ms": tot.kernel_ms}), flush=True)
+
+
 def batched_leg(n=4096, replays=3):
     """Batched workload: n graphs of the batched distribution (seeds 1000..)
     in one persistent launch replayed from a CUDA graph, against one plain
@@ -454,6 +473,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="one reduced launch for ncu: 16 blocks, roots [1000000, 1005000) of the "
                          "large graph (a few GB)")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="one reduced batched launch for ncu: the first 512 graphs of the batch")
     ap.add_argument("--serving-leg", action="store_true",
                     help="run only the serving leg and print its result (used by the N=1 run)")
     args = ap.parse_args()
@@ -462,6 +483,9 @@ def main():
         return
     if args.profile:
         run_profile_case()
+        return
+    if args.profile_batch:
+        run_profile_batch()
         return
     if args.serving_leg:
         print(json.dumps(serving_leg()), flush=True)

@@ -98,7 +98,7 @@ class GenSpec(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_graphs", C.c_int32), ("arena_bytes", C.c_int64),
                 ("max_v", C.c_int32), ("max_degree", C.c_int32), ("max_two_hop", C.c_int32),
-                ("reserved", C.c_int32), ("idle_exit_ns", C.c_int64)]
+                ("prep_threads", C.c_int32), ("idle_exit_ns", C.c_int64)]
 
 
 class ServerStats(C.Structure):
@@ -379,14 +379,14 @@ class Server:
     graphs submitted at any time share one persistent launch."""
 
     def __init__(self, device=0, max_graphs=0, arena_bytes=0, max_v=0, max_degree=0,
-                 max_two_hop=0, idle_exit_ns=0, **params):
+                 max_two_hop=0, idle_exit_ns=0, prep_threads=0, **params):
         self._h = C.c_void_p()
         cfg = ServerConfig()
         _lib.mbe_server_config_default(C.byref(cfg))
         cfg.device = device
         for k, v in dict(max_graphs=max_graphs, arena_bytes=arena_bytes, max_v=max_v,
                          max_degree=max_degree, max_two_hop=max_two_hop,
-                         idle_exit_ns=idle_exit_ns).items():
+                         idle_exit_ns=idle_exit_ns, prep_threads=prep_threads).items():
             if v:
                 setattr(cfg, k, v)
         p = default_params(**params)

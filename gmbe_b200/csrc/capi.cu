@@ -281,22 +281,35 @@ int apply_tuning(const mbe_params& prm, DevGraph* dg) {
   return MBE_OK;
 }
 
+int enum_blocks_per_sm(bool tiers, size_t smem, int* occ) {
+  const void* fn = tiers ? (const void*)mbe_enum_kernel_tiers : (const void*)mbe_enum_kernel;
+  // The limit only ever rises: a server and single-graph launches may share
+  // the kernel from different threads, each with its own bitmap size.
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, fn));
+  if ((size_t)fa.maxDynamicSharedSizeBytes < smem)
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, kEnumThreads, smem));
+  if (*occ < 1) return set_error(MBE_ERR_CUDA, "enumeration kernel cannot be resident");
+  return MBE_OK;
+}
+
 int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm, LaunchPlan* plan) {
   if (!ws.ev0) {
     CK(cudaEventCreate(&ws.ev0));
     CK(cudaEventCreate(&ws.ev1));
   }
-  int dev_sms = 0;
-  CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, spec.device));
-  int occ = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ, spec.n_big > 0 ? mbe_enum_kernel_tiers : mbe_enum_kernel, kEnumThreads, 0));
-  if (occ < 1) return set_error(MBE_ERR_CUDA, "enumeration kernel cannot be resident");
-  plan->blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * occ) : dev_sms * occ;
-  plan->warps = plan->blocks * kEnumWarps;
   if (spec.capC >= (1 << 24))
     return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
   plan->sl = make_layout(spec.map_words, spec.capC, spec.capL, spec.capS);
+  int dev_sms = 0;
+  CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, spec.device));
+  // Every block of the persistent launch is resident at once.
+  int occ = 0;
+  int rc = enum_blocks_per_sm(spec.n_big > 0, enum_smem_bytes(plan->sl), &occ);
+  if (rc) return rc;
+  plan->blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * occ) : dev_sms * occ;
+  plan->warps = plan->blocks * kEnumWarps;
   // The big tier (if any): the first n_big warps.  Both layouts share the
   // count-map size, hence the shared-memory bitmap.
   const int n_big = std::max(0, std::min(spec.n_big, plan->warps));
@@ -307,9 +320,6 @@ int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm,
       return set_error(MBE_ERR_CAPACITY, "candidate sets above 2^24 entries are not supported");
     big_sl = make_layout(spec.map_words, spec.bigC, spec.bigL, spec.bigS);
   }
-  CK(cudaFuncSetAttribute(n_big > 0 ? mbe_enum_kernel_tiers : mbe_enum_kernel,
-                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)enum_smem_bytes(plan->sl)));
   plan->map_words = spec.map_words;
   size_t need = scratch_bytes(plan->sl, big_sl, plan->warps, n_big);
   if (need > ws.scratch_bytes) {
@@ -669,7 +679,11 @@ int plan_two_tiers(mbe_graph* g, const mbe_params& prm, int32_t rb, int32_t re, 
   const int32_t nV = std::max<int32_t>(g->h.V_size, 1);
   int dev_sms = 0, occ = 0;
   CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
+  {
+    const ScratchLayout whole = make_layout(nV, spec->capC, spec->capL, spec->capS);
+    int rc = enum_blocks_per_sm(false, enum_smem_bytes(whole), &occ);
+    if (rc) return rc;
+  }
   const int blocks = prm.blocks > 0 ? std::min(prm.blocks, dev_sms * std::max(occ, 1))
                                     : dev_sms * std::max(occ, 1);
   const int warps = blocks * kEnumWarps;

@@ -124,6 +124,11 @@ inline size_t scratch_bytes(const ScratchLayout& sl, const ScratchLayout& big, i
 // not capturable).  Caller holds ws.mu.
 int engine_prepare(Workspace& ws, const LaunchSpec& spec, const mbe_params& prm, LaunchPlan* plan);
 
+// Resident blocks per SM of the enumeration kernel (the two-tier variant if
+// `tiers`) with `smem` bytes of dynamic shared memory per block; also raises
+// the kernel's dynamic shared memory limit to `smem` where it is lower.
+int enum_blocks_per_sm(bool tiers, size_t smem, int* occ);
+
 // Queues the strided clear of every warp's count map if the layout changed
 // since the maps were last cleared (capturable; a no-op otherwise).
 int engine_clear_maps(Workspace& ws, LaunchPlan* plan, cudaStream_t st);

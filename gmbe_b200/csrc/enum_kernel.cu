@@ -119,6 +119,8 @@ struct Warp {
   uint32_t* seen;                  // this warp's first-touch bitmap in shared memory, or null
   uint64_t deadline;               // %globaltimer after which the launch gives up (0: never)
   uint32_t* gseen;                 // this warp's first-touch bitmap in global memory
+  long long dem_t;                 // clock64 of the last export-demand reading (lane 0)
+  int dem;                         // that reading
 
   __device__ int32_t* A(int64_t off) const { return base + off; }
   __device__ uint64_t* A64(int64_t off) const { return reinterpret_cast<uint64_t*>(base + off); }
@@ -424,16 +426,27 @@ __device__ bool queue_push_one(Warp& W, const Task& t);
 
 // Demand for exported work (lane-uniform): 0 none, 1 idle warps outnumber
 // queued work, 2 more than an eighth of all warps are idle as well.
+// The counters are global loads the warp would wait for on every sizable
+// child, so a reading is reused for kDemandCycles SM clocks (about 2 us):
+// demand moves with warps going idle, far more slowly than children come.
+constexpr long long kDemandCycles = 4096;
 __device__ int export_demand(Warp& W) {
   int want = 0;
   if (lane_id() == 0) {
-    EnumCtl* c = W.ctl;
-    int idle = *(volatile int32_t*)&c->idle_warps;
-    unsigned long long queued = *(volatile unsigned long long*)&c->q_tail -
-                                *(volatile unsigned long long*)&c->q_head;
-    if (idle > 0 && (unsigned long long)idle > queued) {
-      const int warps = (int)(gridDim.x * (blockDim.x >> 5));
-      want = idle > (warps >> 3) ? 2 : 1;
+    const long long now = clock64();
+    if (now - W.dem_t < kDemandCycles) {
+      want = W.dem;
+    } else {
+      EnumCtl* c = W.ctl;
+      int idle = *(volatile int32_t*)&c->idle_warps;
+      unsigned long long queued = *(volatile unsigned long long*)&c->q_tail -
+                                  *(volatile unsigned long long*)&c->q_head;
+      if (idle > 0 && (unsigned long long)idle > queued) {
+        const int warps = (int)(gridDim.x * (blockDim.x >> 5));
+        want = idle > (warps >> 3) ? 2 : 1;
+      }
+      W.dem = want;
+      W.dem_t = now;
     }
   }
   return __shfl_sync(0xffffffffu, want, 0);
@@ -1477,8 +1490,11 @@ __device__ void tier1_run(Warp& W, const T1& t) {
   }
   __syncwarp();
   int level = 1;
+  unsigned steps = 0;
   while (level != 0) {
-    if (must_stop(W)) return;
+    // The stop flag is a global load the whole warp waits for: look at it on
+    // the first step and every 64th after.
+    if ((steps++ & 63u) == 0u && must_stop(W)) return;
     const int end = level == 1 ? t.nend : t.nC;  // the first level may push a part only
     int cur = t1_next_live(bound, ncnt, level_bits(W, level), stack[level - 1], end, level);
     if (cur >= 0) {
@@ -2550,6 +2566,8 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
   W.ns_t1 = W.ns_t2 = W.n_t2 = 0;
   W.pushes = W.shape = 0;
   W.deadline = p.time_limit_ns > 0 ? t_start + (uint64_t)p.time_limit_ns : 0;
+  W.dem = 0;
+  W.dem_t = -(1LL << 62);
   uint64_t ns_idle = 0, n_tasks = 0, max_task = 0, max_info = 0, max_split = 0;
   uint64_t max_pushes = 0, max_shape = 0;
   int32_t max_gid = 0;
@@ -2744,7 +2762,7 @@ __device__ __forceinline__ void enum_main(const DevGraph* graphs, const long lon
   }
 }
 
-__global__ void __launch_bounds__(kEnumThreads, 1)
+__global__ void __launch_bounds__(kEnumThreads, kEnumMinBlocks)
     mbe_enum_kernel(const DevGraph* graphs, const long long* root_prefix,
                     unsigned long long* gres, const __grid_constant__ EnumParams p,
                     const __grid_constant__ ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,
@@ -2753,7 +2771,7 @@ __global__ void __launch_bounds__(kEnumThreads, 1)
   enum_main<false>(graphs, root_prefix, gres, p, sl, ctl, q_tasks, q_seq, pool, scratch, exit_ns);
 }
 
-__global__ void __launch_bounds__(kEnumThreads, 1)
+__global__ void __launch_bounds__(kEnumThreads, kEnumMinBlocks)
     mbe_enum_kernel_tiers(const DevGraph* graphs, const long long* root_prefix,
                           unsigned long long* gres, const __grid_constant__ EnumParams p,
                           const __grid_constant__ ScratchLayout sl, EnumCtl* ctl, Task* q_tasks,

@@ -7,8 +7,16 @@
 
 namespace gmbe {
 
-constexpr int kEnumWarps = 16;                 // warps per block
+#ifndef GMBE_ENUM_WARPS
+#define GMBE_ENUM_WARPS 16
+#endif
+#ifndef GMBE_ENUM_MIN_BLOCKS
+#define GMBE_ENUM_MIN_BLOCKS 1
+#endif
+constexpr int kEnumWarps = GMBE_ENUM_WARPS;    // warps per block
 constexpr int kEnumThreads = kEnumWarps * 32;  // threads per block
+// Blocks per SM the register allocation is made for (launch bounds).
+constexpr int kEnumMinBlocks = GMBE_ENUM_MIN_BLOCKS;
 constexpr int kKMax = 4;                       // bitmap words of the tier-2 sub-problem
 constexpr int kLevelBits = 8;                  // counts-tier levels with a candidate bitmap
 

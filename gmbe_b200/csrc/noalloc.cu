@@ -154,9 +154,9 @@ extern "C" int mbe_enumerate_device_noalloc(const int32_t* d_row_off, const int3
   int fit_blocks = (int)std::min<size_t>((kNoAllocPoolBytes - o_scr) / per_block, kNoAllocMaxBlocks);
   if (fit_blocks < 1)
     return set_error(MBE_ERR_CAPACITY,
-                     "graph needs %zu bytes of scratch per 16-warp block; the no-allocation pool "
+                     "graph needs %zu bytes of scratch per %d-warp block; the no-allocation pool "
                      "holds %zu bytes in total (use mbe_enumerate for graphs this large)",
-                     per_block, kNoAllocPoolBytes);
+                     per_block, kEnumWarps, kNoAllocPoolBytes);
   int sms = 0, occ = 0;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0)) !=

@@ -13,6 +13,12 @@
 // (a launch ends once idle for idle_exit_ns).  Arena blocks are bump-allocated
 // and the arena rewinds only when nothing is resident and no launch runs, so no
 // address is rewritten while a launch may hold it in a cache.
+//
+// Preparation: submit checks the request against the server's capacities
+// from the raw CSR (sizes and degrees only, O(edges)) and copies it; a pool of
+// preparation threads then builds the -t/-o graph, its hash keys and the
+// arena image, so a client that submits many graphs is not held up behind
+// each one's sort and transposes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +27,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -44,11 +51,18 @@ double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-enum ReqState { kWaiting, kResident, kDone, kFailed, kCancelled };
+enum ReqState { kPreparing, kWaiting, kResident, kDone, kFailed, kCancelled };
 
 struct Request {
   uint64_t id = 0;
-  ReqState state = kWaiting;
+  ReqState state = kPreparing;
+  // The submitted CSR, until a preparation thread has built the image.
+  std::vector<int32_t> in_off, in_col;
+  int32_t in_nV = 0, in_nU = 0;
+  mbe_opts opts;
+  bool held = false;    // a preparation thread works on it (outside the lock)
+  bool orphan = false;  // forgotten while held: the preparation thread deletes it
+  std::string msg;      // why it failed, when it failed alone
   std::vector<char> image;  // the arena block; descriptor pointers patched on admission
   size_t bytes = 0;         // image size, a multiple of kBlock
   size_t o_row_off = 0, o_col = 0, o_rev_off = 0, o_rev_col = 0, o_ukey = 0, o_vkey = 0;
@@ -92,7 +106,9 @@ struct mbe_server {
   // Host side, under mu.
   std::mutex mu;
   std::condition_variable cv_loop, cv_done;
-  std::deque<Request*> waiting;
+  std::deque<Request*> preparing;  // submitted, not yet taken by a preparation thread
+  std::set<uint64_t> prep_ids;     // ids submitted and not yet prepared (queued or held)
+  std::deque<Request*> waiting;    // prepared, ascending id
   std::unordered_map<uint64_t, Request*> reqs;
   uint64_t next_id = 1;
   uint64_t published = 0, collected = 0;
@@ -102,6 +118,9 @@ struct mbe_server {
   std::string fatal_msg;
   mbe_server_stats st;
   std::thread loop;
+  std::condition_variable cv_prep;
+  bool prep_stop = false;
+  std::vector<std::thread> prep;
 };
 
 namespace {
@@ -145,13 +164,11 @@ int allocate(mbe_server* s) {
   s->capC = std::max<int32_t>(1, std::min(s->map_words, s->capS));
   int dev_sms = 0, occ = 0;
   SCK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, s->device));
-  SCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mbe_enum_kernel, kEnumThreads, 0));
-  if (occ < 1) return set_error(MBE_ERR_CUDA, "enumeration kernel cannot be resident");
+  s->sl = make_layout(s->map_words, s->capC, s->capL, s->capS);
+  int rc = enum_blocks_per_sm(false, enum_smem_bytes(s->sl), &occ);
+  if (rc) return rc;
   s->blocks = s->prm.blocks > 0 ? std::min(s->prm.blocks, dev_sms * occ) : dev_sms * occ;
   const int warps = s->blocks * kEnumWarps;
-  s->sl = make_layout(s->map_words, s->capC, s->capL, s->capS);
-  SCK(cudaFuncSetAttribute(mbe_enum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)enum_smem_bytes(s->sl)));
   const size_t scratch = (size_t)s->sl.words_per_warp * warps * sizeof(int32_t);
   SCK(cudaMalloc((void**)&s->d_scratch, scratch));
   // Every warp's count map starts all-zero; each task leaves it so.
@@ -243,9 +260,11 @@ void finish(mbe_server* s, Request* r, int rc) {
 void fail_all(mbe_server* s, int rc) {
   for (auto& kv : s->reqs) {
     Request* r = kv.second;
-    if (r->state == kWaiting || r->state == kResident) finish(s, r, rc);
+    if (r->state == kPreparing || r->state == kWaiting || r->state == kResident) finish(s, r, rc);
   }
   s->waiting.clear();
+  s->preparing.clear();
+  s->prep_ids.clear();
   s->resident = 0;
 }
 
@@ -340,9 +359,11 @@ void server_loop(mbe_server* s) {
       s->bump = 0;  // nothing on the device refers to the arena any more
       s->st.arena_resets++;
     }
-    // Admission, first come first served.
+    // Admission, first come first served: not past a request submitted
+    // earlier that is still being prepared.
     while (!s->waiting.empty() && !s->stopping && s->fatal == MBE_OK) {
       Request* r = s->waiting.front();
+      if (!s->prep_ids.empty() && *s->prep_ids.begin() < r->id) break;
       if (s->resident >= s->cfg.max_graphs) break;
       if (s->bump + r->bytes > (size_t)s->cfg.arena_bytes) break;  // rewinds once drained
       s->waiting.pop_front();
@@ -381,7 +402,8 @@ int take(mbe_server* s, uint64_t id, mbe_result* out) {
   if (it == s->reqs.end())
     return set_error(MBE_ERR_NOT_FOUND, "unknown request %llu", (unsigned long long)id);
   Request* r = it->second;
-  if (r->state == kWaiting || r->state == kResident) return MBE_ERR_AGAIN;
+  if (r->state == kPreparing || r->state == kWaiting || r->state == kResident)
+    return MBE_ERR_AGAIN;
   int rc;
   if (r->state == kDone) {
     if (out) *out = r->res;
@@ -389,11 +411,142 @@ int take(mbe_server* s, uint64_t id, mbe_result* out) {
   } else if (r->state == kCancelled) {
     rc = set_error(MBE_ERR_CANCELLED, "request %llu was cancelled", (unsigned long long)id);
   } else {
-    rc = set_error(r->rc, "request %llu failed: %s", (unsigned long long)id, s->fatal_msg.c_str());
+    rc = set_error(r->rc, "request %llu failed: %s", (unsigned long long)id,
+                   r->msg.empty() ? s->fatal_msg.c_str() : r->msg.c_str());
   }
   s->reqs.erase(it);
-  delete r;
+  if (r->held) r->orphan = true;  // its preparation thread deletes it
+  else delete r;
   return rc;
+}
+
+// The server-wide capacities a request must fit, from the raw CSR: the
+// internal V side after -t, its largest degree and its largest two-hop
+// multiset sum_{y in N(x)} d(y).  None depends on the -o row order, so these
+// equal graph_caps() of the built graph.  Also sizes the arena block.
+struct Fit {
+  int32_t V, U, capL, swapped;
+  int64_t capS;
+  size_t o_row_off, o_col, o_rev_off, o_rev_col, o_ukey, o_vkey, bytes;
+};
+
+int fit_of(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t* nU, int64_t nE,
+           const mbe_opts& o, Fit* f) {
+  int32_t maxid = -1;
+  for (int64_t i = 0; i < nE; ++i) maxid = std::max(maxid, col[i]);
+  if (*nU <= 0) *nU = maxid + 1;
+  if (maxid >= *nU) return set_error(MBE_ERR_FORMAT, "U id %d >= nU %d", maxid, *nU);
+  int rc = validate_adj_csr(row_off, col, nV, *nU, nE);
+  if (rc) return rc;
+  if (nE > INT32_MAX) return set_error(MBE_ERR_FORMAT, "more than 2^31-1 edges");
+  const int32_t n_u = *nU;
+  std::vector<int32_t> dcol(n_u, 0);
+  for (int64_t i = 0; i < nE; ++i) dcol[col[i]]++;
+  const bool swap = (o.uvtrans == 1 && n_u < nV) || (o.uvtrans == 2 && n_u > nV);
+  int64_t capS = 0;
+  int32_t capL = 0;
+  if (!swap) {
+    for (int32_t v = 0; v < nV; ++v) {
+      int64_t sum = 0;
+      for (int32_t i = row_off[v]; i < row_off[v + 1]; ++i) sum += dcol[col[i]];
+      capS = std::max(capS, sum);
+      capL = std::max(capL, row_off[v + 1] - row_off[v]);
+    }
+  } else {
+    std::vector<int64_t> sum(n_u, 0);
+    for (int32_t v = 0; v < nV; ++v) {
+      const int32_t d = row_off[v + 1] - row_off[v];
+      for (int32_t i = row_off[v]; i < row_off[v + 1]; ++i) sum[col[i]] += d;
+    }
+    for (int32_t u = 0; u < n_u; ++u) {
+      capS = std::max(capS, sum[u]);
+      capL = std::max(capL, dcol[u]);
+    }
+  }
+  if (capS > INT32_MAX / 2)
+    return set_error(MBE_ERR_CAPACITY, "two-hop multiset of a root exceeds 2^30 entries");
+  f->swapped = swap ? 1 : 0;
+  f->V = swap ? n_u : nV;
+  f->U = swap ? nV : n_u;
+  f->capL = std::max(capL, 1);
+  f->capS = std::max<int64_t>(capS, 1);
+  size_t off = align_up(sizeof(ServeGraph), kArrayAlign);
+  auto place = [&](size_t bytes) {
+    size_t o2 = off;
+    off = align_up(off + std::max<size_t>(bytes, 4), kArrayAlign);
+    return o2;
+  };
+  f->o_row_off = place(sizeof(int32_t) * ((size_t)f->V + 1));
+  f->o_col = place(sizeof(int32_t) * (size_t)nE);
+  f->o_rev_off = place(sizeof(int32_t) * ((size_t)f->U + 1));
+  f->o_rev_col = place(sizeof(int32_t) * (size_t)nE);
+  f->o_ukey = place(sizeof(uint64_t) * (size_t)f->U);
+  f->o_vkey = place(sizeof(uint64_t) * (size_t)f->V);
+  f->bytes = align_up(off, kBlock);
+  return MBE_OK;
+}
+
+// Builds a request's arena image from its submitted CSR (a preparation
+// thread, without the lock).  Writes only into `image`.
+int build_image(const Request* r, std::vector<char>* image) {
+  HostGraph h;
+  int rc = build_host_graph(r->in_off.data(), r->in_col.data(), r->in_nV, r->in_nU,
+                            (int64_t)r->in_col.size(), r->opts, &h);
+  if (rc) return rc;
+  if (h.V_size != r->dg.nV || h.U_size != r->dg.nU || h.swapped != r->dg.swapped)
+    return set_error(MBE_ERR_INVALID, "prepared sides differ from the submitted ones");
+  image->assign(r->bytes, 0);
+  auto put = [&](size_t o2, const void* src, size_t bytes) {
+    if (bytes) memcpy(image->data() + o2, src, bytes);
+  };
+  put(r->o_row_off, h.row_off.data(), sizeof(int32_t) * h.row_off.size());
+  put(r->o_col, h.col.data(), sizeof(int32_t) * h.col.size());
+  put(r->o_rev_off, h.rev_off.data(), sizeof(int32_t) * h.rev_off.size());
+  put(r->o_rev_col, h.rev_col.data(), sizeof(int32_t) * h.rev_col.size());
+  std::vector<uint64_t> uk, vk;
+  host_keys(h, &uk, &vk);
+  put(r->o_ukey, uk.data(), sizeof(uint64_t) * uk.size());
+  put(r->o_vkey, vk.data(), sizeof(uint64_t) * vk.size());
+  return MBE_OK;
+}
+
+// A preparation thread: takes submitted requests in order, builds their
+// images and queues them for admission in id order.
+void prep_loop(mbe_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    s->cv_prep.wait(lk, [&] { return s->prep_stop || !s->preparing.empty(); });
+    if (s->prep_stop) break;
+    Request* r = s->preparing.front();
+    s->preparing.pop_front();
+    r->held = true;
+    lk.unlock();
+    std::vector<char> image;
+    const int rc = build_image(r, &image);
+    const std::string msg = rc ? std::string(mbe_last_error_string()) : std::string();
+    lk.lock();
+    r->held = false;
+    s->prep_ids.erase(r->id);
+    s->cv_loop.notify_one();  // admission may have waited for this one
+    std::vector<int32_t>().swap(r->in_off);
+    std::vector<int32_t>().swap(r->in_col);
+    if (r->orphan) {
+      delete r;
+      continue;
+    }
+    if (r->state != kPreparing) continue;  // cancelled or failed meanwhile
+    if (rc) {
+      r->msg = msg;
+      finish(s, r, rc);
+      continue;
+    }
+    r->image = std::move(image);
+    r->state = kWaiting;
+    auto pos = s->waiting.end();
+    while (pos != s->waiting.begin() && (*(pos - 1))->id > r->id) --pos;
+    s->waiting.insert(pos, r);
+    s->cv_loop.notify_one();
+  }
 }
 
 }  // namespace
@@ -425,7 +578,11 @@ int mbe_server_create(const mbe_server_config* cfg, const mbe_params* params, mb
     if (cfg->max_degree > 0) c.max_degree = cfg->max_degree;
     if (cfg->max_two_hop > 0) c.max_two_hop = cfg->max_two_hop;
     if (cfg->idle_exit_ns > 0) c.idle_exit_ns = cfg->idle_exit_ns;
+    if (cfg->prep_threads > 0) c.prep_threads = cfg->prep_threads;
   }
+  if (c.prep_threads <= 0)
+    c.prep_threads = (int32_t)std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+  if (c.prep_threads > 256) return set_error(MBE_ERR_INVALID, "prep_threads above 256");
   if (c.max_graphs > (1 << 24)) return set_error(MBE_ERR_INVALID, "max_graphs above 2^24");
   if ((c.arena_bytes >> kServeBlockShift) > INT32_MAX)
     return set_error(MBE_ERR_INVALID, "arena above 2^31 blocks");
@@ -442,6 +599,7 @@ int mbe_server_create(const mbe_server_config* cfg, const mbe_params* params, mb
     return rc;
   }
   s->loop = std::thread(server_loop, s);
+  for (int32_t i = 0; i < c.prep_threads; ++i) s->prep.emplace_back(prep_loop, s);
   *out = s;
   return MBE_OK;
 }
@@ -450,70 +608,56 @@ int mbe_server_submit(mbe_server* s, const int32_t* row_off, const int32_t* col,
                       int32_t nU, int64_t nE, const mbe_opts* opts, uint64_t* request_id) {
   clear_error();
   if (!s || !request_id) return set_error(MBE_ERR_INVALID, "null argument");
+  if (nV < 0 || nE < 0 || (nV > 0 && !row_off) || (nE > 0 && !col))
+    return set_error(MBE_ERR_INVALID, "invalid CSR arguments (nV=%d nE=%lld)", nV, (long long)nE);
+  const double t_submit = now_s();
   mbe_opts o;
   if (opts) o = *opts;
   else mbe_opts_default(&o);
-  // Host preparation runs in the caller's thread, outside the server lock.
-  HostGraph h;
-  int rc = build_host_graph(row_off, col, nV, nU, nE, o, &h);
+  Fit f;
+  int rc = fit_of(row_off, col, nV, &nU, nE, o, &f);
   if (rc) return rc;
-  int32_t capL = 1, capS = 1;
-  if ((rc = graph_caps(h, &capL, &capS))) return rc;
   auto reject = [&](const char* what, long long got, long long cap) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->st.rejected++;
     return set_error(MBE_ERR_ADMISSION, "%s %lld exceeds the server's %lld", what, got, cap);
   };
-  if (h.V_size > s->map_words) return reject("internal V side", h.V_size, s->map_words);
-  if (capL > s->capL) return reject("root degree", capL, s->capL);
-  if (capS > s->capS) return reject("two-hop multiset", capS, s->capS);
+  if (f.V > s->map_words) return reject("internal V side", f.V, s->map_words);
+  if (f.capL > s->capL) return reject("root degree", f.capL, s->capL);
+  if (f.capS > s->capS) return reject("two-hop multiset", f.capS, s->capS);
+  if (f.bytes > (size_t)s->cfg.arena_bytes)
+    return reject("graph block bytes", (long long)f.bytes, s->cfg.arena_bytes);
 
   Request* r = new Request();
   DevGraph& g = r->dg;
   memset(&g, 0, sizeof(g));
-  g.nV = h.V_size;
-  g.nU = h.U_size;
-  g.nE = h.edge_size;
-  g.swapped = h.swapped;
-  g.root_end = h.V_size;
+  g.nV = f.V;
+  g.nU = f.U;
+  g.nE = nE;
+  g.swapped = f.swapped;
+  g.root_end = f.V;
   g.root_offset = 0;
   g.root_stride = 1;
-  g.n_roots = h.V_size;
+  g.n_roots = f.V;
   if ((rc = apply_tuning(s->prm, &g))) {
     delete r;
     return rc;
   }
-  size_t off = align_up(sizeof(ServeGraph), kArrayAlign);
-  auto place = [&](size_t bytes) {
-    size_t o2 = off;
-    off = align_up(off + std::max<size_t>(bytes, 4), kArrayAlign);
-    return o2;
-  };
-  r->o_row_off = place(sizeof(int32_t) * h.row_off.size());
-  r->o_col = place(sizeof(int32_t) * h.col.size());
-  r->o_rev_off = place(sizeof(int32_t) * h.rev_off.size());
-  r->o_rev_col = place(sizeof(int32_t) * h.rev_col.size());
-  r->o_ukey = place(sizeof(uint64_t) * (size_t)h.U_size);
-  r->o_vkey = place(sizeof(uint64_t) * (size_t)h.V_size);
-  r->bytes = align_up(off, kBlock);
-  if (r->bytes > (size_t)s->cfg.arena_bytes) {
-    const long long need = (long long)r->bytes;
-    delete r;
-    return reject("graph block bytes", need, s->cfg.arena_bytes);
+  r->o_row_off = f.o_row_off;
+  r->o_col = f.o_col;
+  r->o_rev_off = f.o_rev_off;
+  r->o_rev_col = f.o_rev_col;
+  r->o_ukey = f.o_ukey;
+  r->o_vkey = f.o_vkey;
+  r->bytes = f.bytes;
+  r->opts = o;
+  r->in_nV = nV;
+  r->in_nU = nU;
+  r->t_submit = t_submit;
+  if (f.V > 0) {
+    r->in_off.assign(row_off, row_off + (size_t)nV + 1);
+    r->in_col.assign(col, col + nE);
   }
-  r->image.assign(r->bytes, 0);
-  auto put = [&](size_t o2, const void* src, size_t bytes) {
-    if (bytes) memcpy(r->image.data() + o2, src, bytes);
-  };
-  put(r->o_row_off, h.row_off.data(), sizeof(int32_t) * h.row_off.size());
-  put(r->o_col, h.col.data(), sizeof(int32_t) * h.col.size());
-  put(r->o_rev_off, h.rev_off.data(), sizeof(int32_t) * h.rev_off.size());
-  put(r->o_rev_col, h.rev_col.data(), sizeof(int32_t) * h.rev_col.size());
-  std::vector<uint64_t> uk, vk;
-  host_keys(h, &uk, &vk);
-  put(r->o_ukey, uk.data(), sizeof(uint64_t) * uk.size());
-  put(r->o_vkey, vk.data(), sizeof(uint64_t) * vk.size());
-  r->t_submit = now_s();
 
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stopping) {
@@ -532,8 +676,9 @@ int mbe_server_submit(mbe_server* s, const int32_t* row_off, const int32_t* col,
     s->st.completed++;
     finish(s, r, MBE_OK);
   } else {
-    s->waiting.push_back(r);
-    s->cv_loop.notify_one();
+    s->preparing.push_back(r);
+    s->prep_ids.insert(r->id);
+    s->cv_prep.notify_one();
   }
   *request_id = r->id;
   return MBE_OK;
@@ -569,11 +714,22 @@ int mbe_server_cancel(mbe_server* s, uint64_t request_id) {
   if (it == s->reqs.end())
     return set_error(MBE_ERR_NOT_FOUND, "unknown request %llu", (unsigned long long)request_id);
   Request* r = it->second;
-  if (r->state != kWaiting)
+  if (r->state != kWaiting && r->state != kPreparing)
     return set_error(MBE_ERR_INVALID, "request %llu is already on the GPU or finished",
                      (unsigned long long)request_id);
+  // Out of the queues now: poll may forget it at once (a preparation thread
+  // that holds it deletes it once done).
+  if (r->state == kPreparing) {
+    s->prep_ids.erase(r->id);  // later requests need not wait for it
+    s->cv_loop.notify_one();
+    if (!r->held) {
+      s->preparing.erase(std::remove(s->preparing.begin(), s->preparing.end(), r),
+                         s->preparing.end());
+      std::vector<int32_t>().swap(r->in_off);
+      std::vector<int32_t>().swap(r->in_col);
+    }
+  }
   r->state = kCancelled;
-  // Out of the admission queue now: poll may delete it at once.
   s->waiting.erase(std::remove(s->waiting.begin(), s->waiting.end(), r), s->waiting.end());
   r->image.clear();
   r->image.shrink_to_fit();
@@ -588,7 +744,7 @@ int mbe_server_get_stats(mbe_server* s, mbe_server_stats* out) {
   std::lock_guard<std::mutex> lk(s->mu);
   *out = s->st;
   out->resident = s->resident;
-  out->waiting = (int64_t)s->waiting.size();
+  out->waiting = (int64_t)(s->waiting.size() + s->prep_ids.size());
   out->arena_used = (int64_t)s->bump;
   out->arena_bytes = s->cfg.arena_bytes;
   out->published = s->published;
@@ -642,11 +798,18 @@ int mbe_server_destroy(mbe_server* s) {
     cudaMemcpyAsync(&s->d_sctl->stop, &one, sizeof(one), cudaMemcpyHostToDevice, s->s_copy);
     cudaStreamSynchronize(s->s_copy);
     for (auto& kv : s->reqs)
-      if (kv.second->state == kWaiting || kv.second->state == kResident)
+      if (kv.second->state == kPreparing || kv.second->state == kWaiting ||
+          kv.second->state == kResident)
         finish(s, kv.second, MBE_ERR_CANCELLED);
     s->waiting.clear();
+    s->preparing.clear();
+    s->prep_ids.clear();
+    s->prep_stop = true;
+    s->cv_prep.notify_all();
     s->cv_loop.notify_one();
   }
+  for (std::thread& t : s->prep)
+    if (t.joinable()) t.join();
   if (s->loop.joinable()) s->loop.join();
   release(s);
   delete s;

@@ -356,7 +356,10 @@ typedef struct mbe_server_config {
   int32_t max_v;
   int32_t max_degree;
   int32_t max_two_hop;
-  int32_t reserved;
+  /* Host threads that prepare submitted graphs (the -t/-o build, hash keys
+   * and the arena image) while the GPU runs others (0 = the host's hardware
+   * threads, at most 8). */
+  int32_t prep_threads;
   int64_t idle_exit_ns; /* a launch ends after this long without work (0 = 200 us) */
 } mbe_server_config;
 
@@ -380,11 +383,14 @@ void mbe_server_config_default(mbe_server_config* c);
 /* `params` (may be NULL = defaults) applies to every request. */
 int mbe_server_create(const mbe_server_config* cfg, const mbe_params* params, mbe_server** out);
 
-/* Copies and prepares one .adj-shaped CSR (the -t/-o of `opts`, as in
- * mbe_graph_from_csr) and queues it; returns at once with its id.  Admission
- * (arena space and a graph slot) is first come, first served.  Errors:
- * MBE_ERR_FORMAT / MBE_ERR_INVALID for bad input, MBE_ERR_ADMISSION if the
- * graph exceeds the server's capacities or arena. */
+/* Checks and copies one .adj-shaped CSR and queues it; returns at once with
+ * its id.  The capacity checks run here, in the caller's thread (they need
+ * only the two sides' degrees: the -o order does not change them); the -t/-o
+ * build of `opts`, as in mbe_graph_from_csr, runs on the server's preparation
+ * threads.  Admission (arena space and a graph slot) then follows submission
+ * order among prepared graphs.  Errors: MBE_ERR_FORMAT / MBE_ERR_INVALID for
+ * bad input, MBE_ERR_ADMISSION if the graph exceeds the server's capacities
+ * or arena.  enum_seconds of the result counts from this call. */
 int mbe_server_submit(mbe_server* s, const int32_t* row_off, const int32_t* col, int32_t nV,
                       int32_t nU, int64_t nE, const mbe_opts* opts, uint64_t* request_id);
 

@@ -130,3 +130,46 @@ def test_request_life_cycle(gm):
             srv.cancel(10 ** 9)
         assert ei.value.name == "MBE_ERR_NOT_FOUND"
         assert srv.stats()["cancelled"] == 1
+
+
+def test_preparation_pool_keeps_submission_order_and_exact_results(gm):
+    # Graphs are prepared on the server's own threads (-t/-o build, keys,
+    # arena image) after submit returns; admission still follows submission
+    # order, and every result equals the oracle's, for one preparation thread
+    # and for several.
+    graphs, want = _mix(gm)
+    for threads in (1, 4):
+        with gm.Server(max_v=8192, max_degree=2048, max_two_hop=1 << 17,
+                       prep_threads=threads) as srv:
+            ids = [srv.submit(ro, co, nU) for ro, co, nU in graphs]
+            got = [srv.wait(rid, timeout=120) for rid in ids]
+            st = srv.stats()
+        for i, w in enumerate(want):
+            assert (got[i].count, got[i].set_hash) == w, f"graph {i}, {threads} threads"
+        assert st["completed"] == len(graphs) and st["waiting"] == 0
+
+
+def test_cancel_while_preparing_and_forget_while_held(gm):
+    # A request cancelled before its preparation finished never runs; one
+    # forgotten (polled after cancel) while a preparation thread still holds
+    # it is freed by that thread.  The server stays exact afterwards.
+    big = gm.batch_graph(1007)
+    small = random_bipartite(30, 40, 0.25, 9)
+    w = oracle.gmbe(*small)
+    with gm.Server(max_v=8192, max_degree=2048, max_two_hop=1 << 17, prep_threads=1) as srv:
+        cancelled = 0
+        for _ in range(8):
+            rid = srv.submit(big.row_off, big.col, big.nU)
+            try:
+                srv.cancel(rid)
+                cancelled += 1
+                with pytest.raises(gm.MBEError) as ei:
+                    srv.poll(rid)
+                assert ei.value.name == "MBE_ERR_CANCELLED"
+            except gm.MBEError as e:  # it reached the GPU first
+                assert e.name == "MBE_ERR_INVALID"
+                srv.wait(rid, timeout=120)
+        r = srv.wait(srv.submit(*small), timeout=60)
+        st = srv.stats()
+    assert (r.count, r.set_hash) == (w.count, w.set_hash)
+    assert cancelled >= 1 and st["cancelled"] == cancelled
