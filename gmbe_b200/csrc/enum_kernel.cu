@@ -549,6 +549,14 @@ __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, 
 // shared-array semantics for that pair of levels).  R of the push that
 // opened a level is carried on the stack: absorbed candidates leave the
 // lists but stay in every R below.
+//
+// finder_pop is not a pass of its own: a pop at a level is only remembered
+// (the candidate and the L vertices it leaves, `rem`), and its bound rule is
+// applied record by record by the next pass over the level, the scan for the
+// next candidate and that candidate's push, which write each header once.
+// A level that ends with a pop pending drops it: its records are discarded,
+// or (a list shared with the parent) every bound the pop would set is one
+// the parent's own pop re-derives.
 template <int K>
 __device__ void tier2_run(Warp& W, const T2Src& src) {
   constexpr int RS = K + 1;
@@ -589,6 +597,23 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
   __syncwarp();
   int level = 1;
   unsigned steps = 0;
+  // The pending pop at `level`: its candidate (-1: none) and the L vertices
+  // of the level it does not meet.
+  int pcp = -1;
+  uint32_t prem[K];
+#pragma unroll
+  for (int w = 0; w < K; ++w) prem[w] = 0u;
+  // A record's bound after the pending pop (finder_pop: a bound >= level is
+  // re-derived, FREE if the record meets rem or is the popped one, else
+  // level - 1; without pruning always FREE).
+  auto popped = [&](int q, uint32_t b, const uint32_t* m) -> uint32_t {
+    if (pcp < 0 || (int)b < level) return b;
+    if (!prune || q == pcp) return kB8Free;
+    uint32_t any = 0;
+#pragma unroll
+    for (int w = 0; w < K; ++w) any |= m[w] & prem[w];
+    return any ? kB8Free : (uint32_t)(level - 1);
+  };
   while (level != 0) {
     if ((++steps & 4095u) == 0u && must_stop(W)) return;
     uint32_t* R = reinterpret_cast<uint32_t*>(lrec[level - 1]);
@@ -603,10 +628,13 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
       bool ok = false;
       if (q < e) {
         const uint32_t* r = R + (size_t)q * RS;
-        if ((int)(r[0] & 0xffu) > level - 1) {
+        uint32_t m[K];
+#pragma unroll
+        for (int w = 0; w < K; ++w) m[w] = r[1 + w];
+        if ((int)popped(q, r[0] & 0xffu, m) > level - 1) {
           uint32_t any = 0;
 #pragma unroll
-          for (int w = 0; w < K; ++w) any |= r[1 + w] & Lm[w];
+          for (int w = 0; w < K; ++w) any |= m[w] & Lm[w];
           ok = any != 0;
         }
       }
@@ -664,15 +692,18 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
               cover &= x == Ln[w];
               meet |= x != 0;
             }
-            int b = (int)(h & 0xffu);
+            const uint32_t b0h = h & 0xffu;
+            const int b = (int)popped(q, b0h, mu[u]);
+            uint32_t nb = (uint32_t)b;
             if (cover) {
               sR += subkey[h >> 8];
               ++nR;
               if (q < cp && b >= level) ism = false;
-              else if (b > level) R[(size_t)q * RS] = (h & ~0xffu) | (uint32_t)level;
+              else if (b > level) nb = (uint32_t)level;
             } else {
               keep = meet && b > level;
             }
+            if (nb != b0h) R[(size_t)q * RS] = (h & ~0xffu) | nb;
           }
           unsigned bal = __ballot_sync(kFull, keep);
           if (fits && keep) {
@@ -685,6 +716,7 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
           nbefore += __popc(__ballot_sync(kFull, keep && q < cp));
         }
       }
+      pcp = -1;  // applied by this pass
       ism = __all_sync(kFull, ism);
       sR = warp_sum(sR) + rsum[level - 1];
       nR = warp_sum(nR) + rcnt[level - 1];
@@ -739,46 +771,20 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
       }
       if (lane == 0) lcur[level - 1] = cp + 1;
     } else {
-      --level;
+      --level;  // the ended level's pending pop (if any) is dropped
       if (level == 0) break;
       cp = lcur[level - 1];
       __syncwarp();
       if (lane == 0) lcur[level - 1] = cp + 1;
     }
-    // ---- pop (finder_pop) of the candidate at position cp of `level` ----
+    // ---- pop (finder_pop) of the candidate at position cp of `level`:
+    // remembered, applied by the next pass over the level ----
     {
-      uint32_t* R2 = reinterpret_cast<uint32_t*>(lrec[level - 1]);
-      const int n2 = ln[level - 1];
-      uint32_t rem[K];
+      const uint32_t* R2 = reinterpret_cast<const uint32_t*>(lrec[level - 1]);
+      pcp = cp;
 #pragma unroll
       for (int w = 0; w < K; ++w)
-        rem[w] = lmask[(level - 1) * K + w] & ~R2[(size_t)cp * RS + 1 + w];
-      constexpr int UP = K <= 2 ? 4 : 2;  // records per lane in flight, as in the push
-      for (int q0 = lane; q0 < n2; q0 += 32 * UP) {
-        uint32_t hu[UP], tu[UP];
-#pragma unroll
-        for (int u = 0; u < UP; ++u) {
-          const int q = q0 + u * 32;
-          hu[u] = 0u;
-          tu[u] = 0u;
-          if (q < n2) {
-            const uint32_t* r = R2 + (size_t)q * RS;
-            hu[u] = r[0];
-#pragma unroll
-            for (int w = 0; w < K; ++w) tu[u] |= r[1 + w] & rem[w];
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < UP; ++u) {
-          const int q = q0 + u * 32;
-          const uint32_t h = hu[u];
-          if (q < n2 && (int)(h & 0xffu) >= level) {
-            uint32_t nb = kB8Free;
-            if (prune) nb = (tu[u] != 0 || q == cp) ? kB8Free : (uint32_t)(level - 1);
-            R2[(size_t)q * RS] = (h & ~0xffu) | nb;
-          }
-        }
-      }
+        prem[w] = lmask[(level - 1) * K + w] & ~R2[(size_t)cp * RS + 1 + w];
     }
     __syncwarp();
   }
