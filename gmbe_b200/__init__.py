@@ -160,6 +160,7 @@ _sig = {
     "mbe_server_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
     "mbe_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "mbe_server_destroy": (C.c_int, [C.c_void_p]),
+    "mbe_server_set_emit": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "mbe_server_debug_request": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
 }
 for _name, (_res, _args) in _sig.items():
@@ -207,6 +208,8 @@ def make_opts(uvtrans=0, order=1, fast_mode=1, device=0) -> Opts:
 
 _EMIT_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32), C.c_int32,
                        C.c_void_p)
+_SERVER_EMIT_FN = C.CFUNCTYPE(C.c_int, C.c_uint64, C.POINTER(C.c_int32), C.c_int32,
+                              C.POINTER(C.c_int32), C.c_int32, C.c_void_p)
 
 
 class Graph:
@@ -415,6 +418,8 @@ class Server:
         r = Result()
         ns = -1 if timeout is None else int(timeout * 1e9)
         _check(_lib.mbe_server_wait(self._h, rid, ns, C.byref(r)))
+        if getattr(self, "_emit_err", None):
+            raise self._emit_err.pop(0)
         return r
 
     def cancel(self, rid: int):
@@ -424,6 +429,26 @@ class Server:
         st = ServerStats()
         _check(_lib.mbe_server_get_stats(self._h, C.byref(st)))
         return st.as_dict()
+
+    def set_emit(self, on_biclique, ring_words: int = 0):
+        """mbe_server_set_emit: on_biclique(request id, U ids, V ids) (tuples,
+        original ids) is called on the server's thread for every maximal
+        biclique of every request submitted afterwards; a request's result is
+        reported only after all its bicliques have been passed.  Call before
+        the first submit.  An exception in on_biclique is kept and raised by
+        the next wait()."""
+        self._emit_err = []
+
+        def cb(rid, u, nu, v, nv, _user):
+            try:
+                on_biclique(rid, tuple(u[:nu]), tuple(v[:nv]))
+            except Exception as e:  # noqa: BLE001 - surfaced by wait()
+                self._emit_err.append(e)
+            return 0
+
+        self._emit_cb = _SERVER_EMIT_FN(cb)  # kept alive as long as the server
+        _check(_lib.mbe_server_set_emit(self._h, int(ring_words),
+                                        C.cast(self._emit_cb, C.c_void_p), None))
 
     def debug_request(self, rid: int) -> dict:
         """A resident request's device counters (diagnosis)."""

@@ -902,12 +902,13 @@ int mbe_enumerate(mbe_graph* g, const mbe_params* params, mbe_result* out) {
   return enumerate_graph(g, params, out, nullptr, 0, nullptr);
 }
 
-namespace {
+}  // extern "C"
 
 // One record of the device ring -> the biclique in original ids and sides:
 // L (internal U ids) as given, R = N(L) from the internal U -> V lists.
-void decode_biclique(const HostGraph& h, std::vector<int32_t>& L, std::vector<int32_t>* us,
-                     std::vector<int32_t>* vs, std::vector<int32_t>& R, std::vector<int32_t>& tmp) {
+void gmbe::decode_biclique(const HostGraph& h, std::vector<int32_t>& L, std::vector<int32_t>* us,
+                           std::vector<int32_t>* vs, std::vector<int32_t>& R,
+                           std::vector<int32_t>& tmp) {
   int32_t best = L[0];
   for (int32_t u : L)
     if (h.rev_off[u + 1] - h.rev_off[u] < h.rev_off[best + 1] - h.rev_off[best]) best = u;
@@ -927,7 +928,7 @@ void decode_biclique(const HostGraph& h, std::vector<int32_t>& L, std::vector<in
   std::sort(vs->begin(), vs->end());
 }
 
-}  // namespace
+extern "C" {
 
 extern "C" int mbe_enumerate_emit_stream(mbe_graph* g, const mbe_params* params, mbe_result* out,
                                          int64_t ring_words, mbe_emit_fn fn, void* user) {

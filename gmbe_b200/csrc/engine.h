@@ -163,4 +163,10 @@ void host_keys(const HostGraph& h, std::vector<uint64_t>* uk, std::vector<uint64
 // Capacities of a graph: max |N(v)| and max sum_{u in N(v)} d(u) over roots.
 int graph_caps(const HostGraph& h, int32_t* capL, int32_t* capS);
 
+// One emitted record (L as internal U ids) -> the biclique in original ids
+// and sides, each sorted: R = the common neighbours of L.  R and tmp are
+// scratch.
+void decode_biclique(const HostGraph& h, std::vector<int32_t>& L, std::vector<int32_t>* us,
+                     std::vector<int32_t>* vs, std::vector<int32_t>& R, std::vector<int32_t>& tmp);
+
 }  // namespace gmbe

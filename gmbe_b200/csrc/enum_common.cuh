@@ -141,9 +141,11 @@ struct ServeGraph {
 };
 
 // Completion record, in host-mapped memory; seq = position + 1 once written.
+// emit_end: words of biclique records reserved in this launch when the graph
+// finished; every record of the graph lies below it (emission only).
 struct ServeDone {
-  unsigned long long request, count, hash, non_maximal, seq;
-  unsigned long long pad[3];
+  unsigned long long request, count, hash, non_maximal, seq, emit_end;
+  unsigned long long pad[2];
 };
 
 // Serving state that outlives a launch (device memory).

@@ -2519,6 +2519,9 @@ __device__ void serve_task_done(Warp& W, int32_t gid) {
   d->count = c;
   d->hash = h;
   d->non_maximal = nm;
+  // Every task of the graph reserved its records before it finished, so the
+  // reservation counter now lies past all of them.
+  d->emit_end = *(volatile unsigned long long*)&W.ctl->emit_pos;
   __threadfence_system();
   d->seq = pos + 1;
 }

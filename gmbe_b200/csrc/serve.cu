@@ -19,6 +19,15 @@
 // preparation threads then builds the -t/-o graph, its hash keys and the
 // arena image, so a client that submits many graphs is not held up behind
 // each one's sort and transposes.
+//
+// Emission (mbe_server_set_emit): the launch writes each biclique's L side,
+// tagged with the graph's arena block, into a host-mapped ring; the server
+// thread drains it while the launch runs, decodes each record against the
+// request's prepared graph (kept for this) and hands the biclique to the
+// callback.  A graph's completion record carries the ring position past all
+// of its records, and its result is released only once the drain has passed
+// that position.  The ring restarts from position 0 with every launch, after
+// the launch's last records have been drained.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,6 +35,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <string>
@@ -63,6 +73,7 @@ struct Request {
   bool held = false;    // a preparation thread works on it (outside the lock)
   bool orphan = false;  // forgotten while held: the preparation thread deletes it
   std::string msg;      // why it failed, when it failed alone
+  std::shared_ptr<const HostGraph> hg;  // the prepared graph, kept to decode emitted records
   std::vector<char> image;  // the arena block; descriptor pointers patched on admission
   size_t bytes = 0;         // image size, a multiple of kBlock
   size_t o_row_off = 0, o_col = 0, o_rev_off = 0, o_rev_col = 0, o_ukey = 0, o_vkey = 0;
@@ -121,6 +132,27 @@ struct mbe_server {
   std::condition_variable cv_prep;
   bool prep_stop = false;
   std::vector<std::thread> prep;
+  // Emission (all under mu, drained by the server thread only).
+  mbe_server_emit_fn emit_fn = nullptr;
+  void* emit_user = nullptr;
+  int32_t* h_ring = nullptr;         // host-mapped ring of records [|L|, block, L ids]
+  int32_t* d_ring = nullptr;
+  unsigned long long* h_read = nullptr;  // words consumed, read by the launch
+  unsigned long long* d_read = nullptr;
+  long long ring_cap = 0;
+  unsigned long long ring_pos = 0;   // words taken from the ring in this launch
+  unsigned long long ring_done = 0;  // words whose bicliques the callback has had
+  struct EmitGraph {
+    uint64_t request;
+    std::shared_ptr<const HostGraph> hg;
+  };
+  std::unordered_map<uint32_t, EmitGraph> emit_graphs;  // arena block -> its request
+  struct Finishing {  // completed on the device, records still in the ring
+    uint64_t request;
+    uint32_t blk;
+    unsigned long long emit_end, count, hash, non_maximal;
+  };
+  std::vector<Finishing> finishing;
 };
 
 namespace {
@@ -140,6 +172,8 @@ void release(mbe_server* s) {
   cudaFree(s->d_sctl);
   cudaFree(s->d_arr_blk);
   if (s->h_done) cudaFreeHost(s->h_done);
+  if (s->h_ring) cudaFreeHost(s->h_ring);
+  if (s->h_read) cudaFreeHost(s->h_read);
   cudaFree(s->d_ctl);
   cudaFree(s->d_q_tasks);
   cudaFree(s->d_q_seq);
@@ -266,6 +300,8 @@ void fail_all(mbe_server* s, int rc) {
   s->preparing.clear();
   s->prep_ids.clear();
   s->resident = 0;
+  s->finishing.clear();
+  s->emit_graphs.clear();
 }
 
 // Copies one admitted graph into the arena and publishes it (server thread,
@@ -302,6 +338,7 @@ int admit(mbe_server* s, Request* r, std::unique_lock<std::mutex>& lk) {
   s->st.admitted++;
   r->state = kResident;
   const uint32_t blk = (uint32_t)(off >> kServeBlockShift);
+  if (s->emit_fn) s->emit_graphs[blk] = mbe_server::EmitGraph{r->id, std::move(r->hg)};
   const unsigned long long tail = s->published;
   lk.unlock();
   cudaError_t e = cudaMemcpyAsync(base, image.data(), bytes, cudaMemcpyHostToDevice, s->s_copy);
@@ -317,36 +354,138 @@ int admit(mbe_server* s, Request* r, std::unique_lock<std::mutex>& lk) {
   return MBE_OK;
 }
 
+// Releases a request's result (caller holds mu).
+void complete(mbe_server* s, uint64_t id, unsigned long long count, unsigned long long hash,
+              unsigned long long non_maximal) {
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end() || it->second->state != kResident) return;
+  Request* r = it->second;
+  memset(&r->res, 0, sizeof(r->res));
+  r->res.count = count;
+  r->res.set_hash = hash;
+  r->res.non_maximal = non_maximal;
+  r->res.enum_seconds = now_s() - r->t_submit;
+  s->st.completed++;
+  finish(s, r, MBE_OK);
+}
+
+// Completions whose records have all been handed to the callback (all of
+// them when `all`: the launch has ended and its ring is drained).
+void release_finished(mbe_server* s, bool all) {
+  auto keep = s->finishing.begin();
+  for (auto it = s->finishing.begin(); it != s->finishing.end(); ++it) {
+    if (all || it->emit_end <= s->ring_done) {
+      complete(s, it->request, it->count, it->hash, it->non_maximal);
+      s->emit_graphs.erase(it->blk);
+    } else {
+      *keep++ = *it;
+    }
+  }
+  s->finishing.erase(keep, s->finishing.end());
+}
+
+// Takes every committed record off the ring and hands its biclique to the
+// callback, with the lock released while decoding and calling (caller holds
+// mu through `lk`; only the server thread drains).  True if any was taken.
+bool drain_emission(mbe_server* s, std::unique_lock<std::mutex>& lk) {
+  struct Rec {
+    uint64_t request;
+    std::shared_ptr<const HostGraph> hg;
+    std::vector<int32_t> L;
+  };
+  std::vector<Rec> batch;
+  volatile int32_t* ring = s->h_ring;
+  const unsigned long long cap = (unsigned long long)s->ring_cap;
+  const unsigned long long start = s->ring_pos;
+  while (true) {
+    const int32_t len = ring[s->ring_pos % cap];
+    if (len <= 0) break;
+    const uint32_t blk = (uint32_t)ring[(s->ring_pos + 1) % cap];
+    Rec rec;
+    rec.L.resize((size_t)len);
+    for (int32_t i = 0; i < len; ++i) rec.L[i] = ring[(s->ring_pos + 2 + i) % cap];
+    for (int32_t i = 0; i < len + 2; ++i) ring[(s->ring_pos + i) % cap] = 0;
+    s->ring_pos += (unsigned long long)len + 2;
+    *(volatile unsigned long long*)s->h_read = s->ring_pos;
+    auto it = s->emit_graphs.find(blk);
+    if (it != s->emit_graphs.end()) {
+      rec.request = it->second.request;
+      rec.hg = it->second.hg;
+      batch.push_back(std::move(rec));
+    }
+  }
+  if (!batch.empty()) {
+    lk.unlock();
+    std::vector<int32_t> us, vs, R, tmp;
+    for (Rec& b : batch) {
+      decode_biclique(*b.hg, b.L, &us, &vs, R, tmp);
+      s->emit_fn(b.request, us.data(), (int32_t)us.size(), vs.data(), (int32_t)vs.size(),
+                 s->emit_user);
+    }
+    lk.lock();
+  }
+  s->ring_done = s->ring_pos;
+  return s->ring_pos != start;
+}
+
+// Completion records, in the order the device handed out their positions
+// (caller holds mu).  True if any was taken.
+bool collect_completions(mbe_server* s) {
+  bool any = false;
+  while (true) {
+    volatile ServeDone* d = s->h_done + (s->collected % (uint64_t)s->done_cap);
+    if (d->seq != s->collected + 1) break;
+    const uint64_t id = d->request;
+    auto it = s->reqs.find(id);
+    if (it != s->reqs.end() && it->second->state == kResident) {
+      if (s->emit_fn) {
+        // Released once the drain has passed the graph's records.
+        s->finishing.push_back(mbe_server::Finishing{
+            id, (uint32_t)(it->second->arena_off >> kServeBlockShift), d->emit_end, d->count,
+            d->hash, d->non_maximal});
+      } else {
+        complete(s, id, d->count, d->hash, d->non_maximal);
+      }
+    }
+    s->collected++;
+    s->resident--;
+    any = true;
+  }
+  return any;
+}
+
 void server_loop(mbe_server* s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
     bool progress = false;
-    // Completion records, in the order the device handed out their positions.
-    while (true) {
-      volatile ServeDone* d = s->h_done + (s->collected % (uint64_t)s->done_cap);
-      if (d->seq != s->collected + 1) break;
-      const uint64_t id = d->request;
-      auto it = s->reqs.find(id);
-      if (it != s->reqs.end() && it->second->state == kResident) {
-        Request* r = it->second;
-        memset(&r->res, 0, sizeof(r->res));
-        r->res.count = d->count;
-        r->res.set_hash = d->hash;
-        r->res.non_maximal = d->non_maximal;
-        r->res.enum_seconds = now_s() - r->t_submit;
-        s->st.completed++;
-        finish(s, r, MBE_OK);
-      }
-      s->collected++;
-      s->resident--;
-      progress = true;
+    if (s->emit_fn && s->fatal == MBE_OK) {
+      progress |= drain_emission(s, lk);
+      release_finished(s, false);
     }
+    progress |= collect_completions(s);
+    if (s->emit_fn) release_finished(s, false);
     // A launch that ended.
     if (s->running && cudaEventQuery(s->ev_run) == cudaSuccess) {
       s->running = false;
       EnumCtl ctl;
       cudaError_t e = cudaMemcpy(&ctl, s->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost);
+      if (e == cudaSuccess && ctl.status == 0 && s->emit_fn) {
+        // Completions written just before the end, then every record of the
+        // launch (all committed now); the ring restarts with the next launch.
+        collect_completions(s);
+        while (s->ring_pos < ctl.emit_pos && drain_emission(s, lk)) {
+        }
+        if (s->ring_pos == ctl.emit_pos) {
+          release_finished(s, true);
+          s->ring_pos = s->ring_done = 0;
+          *(volatile unsigned long long*)s->h_read = 0;
+        } else if (!s->stopping) {
+          s->fatal = MBE_ERR_CUDA;
+          s->fatal_msg = "emission ring: records reserved but never written";
+          fail_all(s, s->fatal);
+        }
+      }
       if (e != cudaSuccess || ctl.status != 0) {
         s->fatal = e != cudaSuccess ? MBE_ERR_CUDA
                                     : (ctl.status == kStCapacity ? MBE_ERR_CAPACITY : MBE_ERR_TIMEOUT);
@@ -487,8 +626,9 @@ int fit_of(const int32_t* row_off, const int32_t* col, int32_t nV, int32_t* nU, 
 }
 
 // Builds a request's arena image from its submitted CSR (a preparation
-// thread, without the lock).  Writes only into `image`.
-int build_image(const Request* r, std::vector<char>* image) {
+// thread, without the lock).  Writes only into `image`, and into `keep` (the
+// prepared graph, for decoding emitted records) when it is not null.
+int build_image(const Request* r, std::vector<char>* image, HostGraph* keep) {
   HostGraph h;
   int rc = build_host_graph(r->in_off.data(), r->in_col.data(), r->in_nV, r->in_nU,
                             (int64_t)r->in_col.size(), r->opts, &h);
@@ -507,6 +647,7 @@ int build_image(const Request* r, std::vector<char>* image) {
   host_keys(h, &uk, &vk);
   put(r->o_ukey, uk.data(), sizeof(uint64_t) * uk.size());
   put(r->o_vkey, vk.data(), sizeof(uint64_t) * vk.size());
+  if (keep) *keep = std::move(h);
   return MBE_OK;
 }
 
@@ -522,7 +663,8 @@ void prep_loop(mbe_server* s) {
     r->held = true;
     lk.unlock();
     std::vector<char> image;
-    const int rc = build_image(r, &image);
+    std::shared_ptr<HostGraph> hg = s->emit_fn ? std::make_shared<HostGraph>() : nullptr;
+    const int rc = build_image(r, &image, hg.get());
     const std::string msg = rc ? std::string(mbe_last_error_string()) : std::string();
     lk.lock();
     r->held = false;
@@ -541,6 +683,7 @@ void prep_loop(mbe_server* s) {
       continue;
     }
     r->image = std::move(image);
+    r->hg = std::move(hg);
     r->state = kWaiting;
     auto pos = s->waiting.end();
     while (pos != s->waiting.begin() && (*(pos - 1))->id > r->id) --pos;
@@ -738,6 +881,46 @@ int mbe_server_cancel(mbe_server* s, uint64_t request_id) {
   return MBE_OK;
 }
 
+int mbe_server_set_emit(mbe_server* s, int64_t ring_words, mbe_server_emit_fn fn, void* user) {
+  clear_error();
+  if (!s || !fn || ring_words < 0) return set_error(MBE_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->emit_fn || s->st.submitted > 0)
+    return set_error(MBE_ERR_INVALID, "emission is set once, before the first submit");
+  // The ring holds at least one record of the largest L (a root's degree).
+  const long long cap =
+      std::max<long long>({ring_words > 0 ? ring_words : (long long)1 << 22,
+                           (long long)s->capL + 2, 64});
+  SCK(cudaSetDevice(s->device));
+  int32_t* h_ring = nullptr;
+  unsigned long long* h_read = nullptr;
+  cudaError_t e = cudaHostAlloc((void**)&h_ring, sizeof(int32_t) * (size_t)cap, cudaHostAllocMapped);
+  if (e == cudaSuccess)
+    e = cudaHostAlloc((void**)&h_read, sizeof(unsigned long long), cudaHostAllocMapped);
+  if (e == cudaSuccess) {
+    memset(h_ring, 0, sizeof(int32_t) * (size_t)cap);
+    *h_read = 0;
+    e = cudaHostGetDevicePointer((void**)&s->d_ring, h_ring, 0);
+  }
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->d_read, h_read, 0);
+  if (e != cudaSuccess) {
+    if (h_ring) cudaFreeHost(h_ring);
+    if (h_read) cudaFreeHost(h_read);
+    s->d_ring = nullptr;
+    s->d_read = nullptr;
+    return set_error(MBE_ERR_NOMEM, "emission ring of %lld words: %s", cap, cudaGetErrorString(e));
+  }
+  s->h_ring = h_ring;
+  s->h_read = h_read;
+  s->ring_cap = cap;
+  s->ep.emit = s->d_ring;
+  s->ep.emit_cap = cap;
+  s->ep.emit_read = s->d_read;
+  s->emit_user = user;
+  s->emit_fn = fn;
+  return MBE_OK;
+}
+
 int mbe_server_get_stats(mbe_server* s, mbe_server_stats* out) {
   clear_error();
   if (!s || !out) return set_error(MBE_ERR_INVALID, "null argument");
@@ -796,6 +979,9 @@ int mbe_server_destroy(mbe_server* s) {
     int32_t one = 1;
     cudaSetDevice(s->device);
     cudaMemcpyAsync(&s->d_sctl->stop, &one, sizeof(one), cudaMemcpyHostToDevice, s->s_copy);
+    // Also ends a wait for room in the emission ring, which looks only at abort.
+    if (s->emit_fn)
+      cudaMemcpyAsync(&s->d_ctl->abort, &one, sizeof(one), cudaMemcpyHostToDevice, s->s_copy);
     cudaStreamSynchronize(s->s_copy);
     for (auto& kv : s->reqs)
       if (kv.second->state == kPreparing || kv.second->state == kWaiting ||

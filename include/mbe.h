@@ -414,6 +414,22 @@ int mbe_server_get_stats(mbe_server* s, mbe_server_stats* out);
  * MBE_ERR_INVALID if the request is not on the device. */
 int mbe_server_debug_request(mbe_server* s, uint64_t request_id, uint64_t out[4]);
 
+/* Biclique lists from the server (no counterpart in the reference, which
+ * only counts): every maximal biclique of every request, in original ids and
+ * sides, each side ascending, with the request it belongs to.  The return
+ * value is ignored. */
+typedef int (*mbe_server_emit_fn)(uint64_t request_id, const int32_t* u_ids, int32_t n_u,
+                                  const int32_t* v_ids, int32_t n_v, void* user);
+
+/* Turns on emission for every request submitted afterwards; call it before
+ * the first submit (MBE_ERR_INVALID after).  Records pass through a
+ * host-mapped ring of `ring_words` int32 words (at least max_degree + 2; 0 =
+ * 2^22) that the server thread drains while the launch runs, calling `fn`
+ * on that thread; a launch whose ring is full waits for it.  A request's
+ * result (mbe_server_poll / wait) is reported only after all its bicliques
+ * have been passed to `fn`. */
+int mbe_server_set_emit(mbe_server* s, int64_t ring_words, mbe_server_emit_fn fn, void* user);
+
 /* Stops the launch (graphs still on the GPU are abandoned) and frees all. */
 int mbe_server_destroy(mbe_server* s);
 

@@ -173,3 +173,41 @@ def test_cancel_while_preparing_and_forget_while_held(gm):
         st = srv.stats()
     assert (r.count, r.set_hash) == (w.count, w.set_hash)
     assert cancelled >= 1 and st["cancelled"] == cancelled
+
+
+def test_server_emission_gives_every_biclique_before_the_result(gm):
+    # mbe_server_set_emit: the bicliques of every request, drained from the
+    # launch's ring by the server thread, equal mbe_enumerate_emit_stream's
+    # for the same graph (as sets; each once), and all of a request's have
+    # been delivered when its result comes back.  A ring of 4,096 words is
+    # far smaller than the output, so the launch waits for the drain.
+    graphs = [random_bipartite(64, 48, 0.3, 11), planted(300, 200, blocks=6, seed=13, bsize=14),
+              hub_graph(3), random_bipartite(120, 90, 0.08, 102)]
+    for seed in (1000, 1002, 1004, 1007):
+        g = gm.batch_graph(seed)
+        graphs.append((g.row_off, g.col, g.nU))
+    want = []
+    for ro, co, nU in graphs:
+        got = []
+        with gm.Graph.from_csr(ro, co, nU, uvtrans=1, order=1, fast_mode=1) as G:
+            r = G.enumerate_stream(lambda u, v: got.append((u, v)) and False)
+        want.append((sorted(got), r.count, r.set_hash))
+    for ring in (4096, 0):
+        with gm.Server(max_v=8192, max_degree=2048, max_two_hop=1 << 17) as srv:
+            recs = {}
+            seen_at_result = {}
+            srv.set_emit(lambda rid, u, v: recs.setdefault(rid, []).append((u, v)),
+                         ring_words=ring)
+            ids = [srv.submit(ro, co, nU) for ro, co, nU in graphs]
+            res = []
+            for rid in ids:
+                res.append(srv.wait(rid, timeout=120))
+                seen_at_result[rid] = len(recs.get(rid, []))
+            with pytest.raises(gm.MBEError) as ei:
+                srv.set_emit(lambda *a: None)  # only before the first submit
+            assert ei.value.name == "MBE_ERR_INVALID"
+        for i, rid in enumerate(ids):
+            bic, count, h = want[i]
+            assert (res[i].count, res[i].set_hash) == (count, h), (ring, i)
+            assert seen_at_result[rid] == count, (ring, i)
+            assert sorted(recs[rid]) == bic, (ring, i)
