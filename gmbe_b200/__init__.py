@@ -161,6 +161,7 @@ _sig = {
     "mbe_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "mbe_server_destroy": (C.c_int, [C.c_void_p]),
     "mbe_server_set_emit": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "mbe_measure_l2_read": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, C.POINTER(C.c_double)]),
     "mbe_server_debug_request": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
 }
 for _name, (_res, _args) in _sig.items():
@@ -540,3 +541,11 @@ def read_adj(path: str) -> BipartiteCSR:
 
 
 from .configs import CONFIGS, DESCRIPTIONS, batch_graph, config_graph  # noqa: E402,F401
+
+
+def measure_l2_read(device: int = 0, nbytes: int = 32 << 20, passes: int = 100) -> float:
+    """mbe_measure_l2_read: GB/s of L2-resident reads (one launch, `passes`
+    sweeps over an `nbytes` buffer with L1-bypassing loads)."""
+    out = C.c_double()
+    _check(_lib.mbe_measure_l2_read(device, nbytes, passes, C.byref(out)))
+    return out.value

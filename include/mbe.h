@@ -433,6 +433,14 @@ int mbe_server_set_emit(mbe_server* s, int64_t ring_words, mbe_server_emit_fn fn
 /* Stops the launch (graphs still on the GPU are abandoned) and frees all. */
 int mbe_server_destroy(mbe_server* s);
 
+/* ---- measurement (no counterpart in the reference) ------------------------
+ * L2 read bandwidth as the SMs see it, for the benchmark's roofline of
+ * workloads whose graph fits L2: one launch reads a `bytes` buffer (1-96
+ * MiB, device memory it allocates and frees) `passes` (1-1000) times with loads that
+ * bypass L1, after a warm-up sweep has brought it into L2; *gbs = bytes read
+ * per second / 1e9, timed with CUDA events. */
+int mbe_measure_l2_read(int32_t device, int64_t bytes, int32_t passes, double* gbs);
+
 /* ---- synthetic inputs ------------------------------------------------------
  * Seeded Chung-Lu bipartite generator (splitmix64 stream, Vose alias
  * sampling): expected degree of vertex i proportional to (i+1)^(-1/(gamma-1)),

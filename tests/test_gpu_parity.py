@@ -262,3 +262,12 @@ def test_share_counts_switch_and_device_release(gm):
             gm.release_device(0)
         r = G.enumerate()
         assert (r.count, r.set_hash) == (want.count, want.set_hash)
+
+
+def test_l2_read_measurement(gm):
+    # The benchmark's L2 roofline denominator: reads of an L2-resident buffer
+    # run well above HBM speed (B200: HBM ~6.5 TB/s measured by copy).
+    gbs = gm.measure_l2_read(0, 32 << 20, 50)
+    assert 5000 < gbs < 200000
+    with pytest.raises(gm.MBEError):
+        gm.measure_l2_read(0, 1 << 10, 50)
