@@ -627,11 +627,20 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
       int q = b0 + lane;
       bool ok = false;
       if (q < e) {
-        const uint32_t* r = R + (size_t)q * RS;
-        uint32_t m[K];
+        uint32_t h, m[K];
+        if constexpr (K == 1) {
+          // One 8-byte load per record (lists start 8-byte aligned, records
+          // are two words): half the load instructions and L1 wavefronts.
+          const uint2 hm = reinterpret_cast<const uint2*>(R)[q];
+          h = hm.x;
+          m[0] = hm.y;
+        } else {
+          const uint32_t* r = R + (size_t)q * RS;
+          h = r[0];
 #pragma unroll
-        for (int w = 0; w < K; ++w) m[w] = r[1 + w];
-        if ((int)popped(q, r[0] & 0xffu, m) > level - 1) {
+          for (int w = 0; w < K; ++w) m[w] = r[1 + w];
+        }
+        if ((int)popped(q, h & 0xffu, m) > level - 1) {
           uint32_t any = 0;
 #pragma unroll
           for (int w = 0; w < K; ++w) any |= m[w] & Lm[w];
@@ -673,10 +682,16 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
 #pragma unroll
           for (int w = 0; w < K; ++w) mu[u][w] = 0u;
           if (q < n) {
-            const uint32_t* r = R + (size_t)q * RS;
-            hu[u] = r[0];
+            if constexpr (K == 1) {
+              const uint2 hm = reinterpret_cast<const uint2*>(R)[q];
+              hu[u] = hm.x;
+              mu[u][0] = hm.y;
+            } else {
+              const uint32_t* r = R + (size_t)q * RS;
+              hu[u] = r[0];
 #pragma unroll
-            for (int w = 0; w < K; ++w) mu[u][w] = r[1 + w];
+              for (int w = 0; w < K; ++w) mu[u][w] = r[1 + w];
+            }
           }
         }
 #pragma unroll
@@ -707,10 +722,15 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
           }
           unsigned bal = __ballot_sync(kFull, keep);
           if (fits && keep) {
-            uint32_t* c = child + (size_t)(nchild + __popc(bal & lanemask_lt())) * RS;
-            c[0] = (h & ~0xffu) | kB8Free;
+            const int ci = nchild + __popc(bal & lanemask_lt());
+            if constexpr (K == 1) {
+              reinterpret_cast<uint2*>(child)[ci] = make_uint2((h & ~0xffu) | kB8Free, mu[u][0]);
+            } else {
+              uint32_t* c = child + (size_t)ci * RS;
+              c[0] = (h & ~0xffu) | kB8Free;
 #pragma unroll
-            for (int w = 0; w < K; ++w) c[1 + w] = mu[u][w];
+              for (int w = 0; w < K; ++w) c[1 + w] = mu[u][w];
+            }
           }
           nchild += __popc(bal);
           nbefore += __popc(__ballot_sync(kFull, keep && q < cp));
