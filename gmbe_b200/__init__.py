@@ -438,18 +438,21 @@ class Server:
         reported only after all its bicliques have been passed.  Call before
         the first submit.  An exception in on_biclique is kept and raised by
         the next wait()."""
-        self._emit_err = []
+        errs = []
 
         def cb(rid, u, nu, v, nv, _user):
             try:
                 on_biclique(rid, tuple(u[:nu]), tuple(v[:nv]))
             except Exception as e:  # noqa: BLE001 - surfaced by wait()
-                self._emit_err.append(e)
+                errs.append(e)
             return 0
 
-        self._emit_cb = _SERVER_EMIT_FN(cb)  # kept alive as long as the server
-        _check(_lib.mbe_server_set_emit(self._h, int(ring_words),
-                                        C.cast(self._emit_cb, C.c_void_p), None))
+        f = _SERVER_EMIT_FN(cb)
+        _check(_lib.mbe_server_set_emit(self._h, int(ring_words), C.cast(f, C.c_void_p), None))
+        # Only a callback the server took is kept (alive as long as the server);
+        # a refused call leaves the one in use untouched.
+        self._emit_cb = f
+        self._emit_err = errs
 
     def debug_request(self, rid: int) -> dict:
         """A resident request's device counters (diagnosis)."""
