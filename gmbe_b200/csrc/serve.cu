@@ -397,7 +397,9 @@ bool drain_emission(mbe_server* s, std::unique_lock<std::mutex>& lk) {
   volatile int32_t* ring = s->h_ring;
   const unsigned long long cap = (unsigned long long)s->ring_cap;
   const unsigned long long start = s->ring_pos;
-  while (true) {
+  // At most one ring's worth per call: the lock is held while records are
+  // taken, and a launch may refill the ring as fast as it is emptied.
+  while (s->ring_pos - start < cap) {
     const int32_t len = ring[s->ring_pos % cap];
     if (len <= 0) break;
     const uint32_t blk = (uint32_t)ring[(s->ring_pos + 1) % cap];
