@@ -328,13 +328,19 @@ __device__ __forceinline__ void graph_spawned(const Warp& W, unsigned long long 
 // Bitmap sub-problems.
 //
 // A sub-problem is an L of at most 128 vertices (K = 1, 2 or 4 words) and a
-// list of candidate records of K+1 words: word 0 = (index << 8) | bound,
+// list of candidate records of rec_stride(K) words: word 0 = (index << 8) | bound,
 // words 1..K = the candidate's neighbourhood inside L.  index is the
 // candidate's position in the sub-problem, whose order is [Q | P]; bound is
 // GMBE's level bound in 8 bits (kB8Free = live at every level; levels stay
 // at or below 129).  subkey[index] is the candidate's hash key, lkey[b] that
 // of L bit b.
 constexpr uint32_t kB8Free = 255;
+// Words per record: K + 1, except that K = 2 records are padded to 4 words so
+// that one 16-byte access reads or writes a record (one-word records are one
+// 8-byte access).  Lists start at 32-byte aligned scratch slices or slots and
+// follow one another in whole records, so K = 1 and K = 2 lists stay 8- and
+// 16-byte aligned.
+__host__ __device__ constexpr int rec_stride(int K) { return K == 2 ? 4 : K + 1; }
 
 struct T2Src {
   uint32_t* rec;           // nsub records, writable (their bounds change)
@@ -355,17 +361,17 @@ constexpr int kSlotLkey = kSlotHdr;
 constexpr int kSlotLid = kSlotLkey + 2 * 32 * 4;  // 128 int32: the L bits' vertex ids
 constexpr int kSlotRec = kSlotLid + 32 * 4;
 __host__ __device__ constexpr int slot_cap(int K) {
-  return ((kSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
+  return ((kSlotWords - kSlotRec - 2) / (rec_stride(K) + 2)) & ~31;
 }
 __host__ __device__ constexpr int big_slot_cap(int K) {
-  return ((kBigSlotWords - kSlotRec - 2) / (K + 3)) & ~31;
+  return ((kBigSlotWords - kSlotRec - 2) / (rec_stride(K) + 2)) & ~31;
 }
 static_assert(slot_cap(1) == kSlotMaxRecords && slot_cap(1) >= slot_cap(2) &&
                   slot_cap(2) >= slot_cap(4) && kSlotWords == kSlotWordsHost,
               "host view of the slot size");
 // header words: 0 K, 1 nsub, 2 nq, 3 graph, 4..7 L0, 8..9 sR0, 10 nR0
 __device__ __forceinline__ uint64_t* slot_subkey(int32_t* sp, int K, int nsub) {
-  return reinterpret_cast<uint64_t*>(sp + kSlotRec + ((nsub * (K + 1) + 1) & ~1));
+  return reinterpret_cast<uint64_t*>(sp + kSlotRec + ((nsub * rec_stride(K) + 1) & ~1));
 }
 
 // Claims a free slot of an occupancy bitmap of n slots (lane 0); -1 if none.
@@ -513,7 +519,7 @@ __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, 
   int slot = lane == 0 ? slot_alloc_for(W, nchild, K) : 0;
   slot = __shfl_sync(0xffffffffu, slot, 0);
   if (slot < 0) return false;
-  constexpr int RS = K + 1;
+  constexpr int RS = rec_stride(K);
   int32_t* sp = slot_ptr(W, slot);
   uint32_t* rec = reinterpret_cast<uint32_t*>(sp + kSlotRec);
   uint64_t* key = slot_subkey(sp, K, nchild);
@@ -559,7 +565,7 @@ __device__ bool t2_try_export(Warp& W, const T2Src& src, const uint32_t* child, 
 // the parent's own pop re-derives.
 template <int K>
 __device__ void tier2_run(Warp& W, const T2Src& src) {
-  constexpr int RS = K + 1;
+  constexpr int RS = rec_stride(K);
   const int lane = (int)lane_id();
   const uint64_t* subkey = src.subkey;
   const uint64_t* lkey = src.lkey;
@@ -634,6 +640,11 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
           const uint2 hm = reinterpret_cast<const uint2*>(R)[q];
           h = hm.x;
           m[0] = hm.y;
+        } else if constexpr (K == 2) {
+          const uint4 hm = reinterpret_cast<const uint4*>(R)[q];  // padded to 4 words
+          h = hm.x;
+          m[0] = hm.y;
+          m[1] = hm.z;
         } else {
           const uint32_t* r = R + (size_t)q * RS;
           h = r[0];
@@ -686,6 +697,11 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
               const uint2 hm = reinterpret_cast<const uint2*>(R)[q];
               hu[u] = hm.x;
               mu[u][0] = hm.y;
+            } else if constexpr (K == 2) {
+              const uint4 hm = reinterpret_cast<const uint4*>(R)[q];
+              hu[u] = hm.x;
+              mu[u][0] = hm.y;
+              mu[u][1] = hm.z;
             } else {
               const uint32_t* r = R + (size_t)q * RS;
               hu[u] = r[0];
@@ -725,6 +741,9 @@ __device__ void tier2_run(Warp& W, const T2Src& src) {
             const int ci = nchild + __popc(bal & lanemask_lt());
             if constexpr (K == 1) {
               reinterpret_cast<uint2*>(child)[ci] = make_uint2((h & ~0xffu) | kB8Free, mu[u][0]);
+            } else if constexpr (K == 2) {
+              reinterpret_cast<uint4*>(child)[ci] =
+                  make_uint4((h & ~0xffu) | kB8Free, mu[u][0], mu[u][1], 0u);
             } else {
               uint32_t* c = child + (size_t)ci * RS;
               c[0] = (h & ~0xffu) | kB8Free;
@@ -867,7 +886,7 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   for (int w = 0; w < 4; ++w) src.L0[w] = (uint32_t)vh[4 + w];
   src.sR0 = (uint64_t)(uint32_t)vh[8] | ((uint64_t)(uint32_t)vh[9] << 32);
   src.nR0 = (uint32_t)vh[10];
-  const int RS = K + 1;
+  const int RS = rec_stride(K);
   uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
   uint64_t* subkey = W.A64(W.sl.sub_v);
   uint64_t* lkey = W.A64(W.sl.lkey);
@@ -898,10 +917,10 @@ __device__ void tier2_from_slot(Warp& W, int slot) {
   tier2_dispatch(W, src, K);
 }
 
-// Zeroes nsub records of K+1 words, each with its index and a free bound.
+// Zeroes nsub records of K mask words, each with its index and a free bound.
 __device__ void init_records(uint32_t* rec, int K, int nsub) {
   const int lane = (int)lane_id();
-  const int RS = K + 1;
+  const int RS = rec_stride(K);
   for (int q = lane; q < nsub; q += 32) {
     rec[(size_t)q * RS] = ((uint32_t)q << 8) | kB8Free;
     for (int w = 0; w < K; ++w) rec[(size_t)q * RS + 1 + w] = 0u;
@@ -1095,7 +1114,7 @@ __device__ void t1_handoff(Warp& W, const T1& t, int x, int level, int kept, uin
   }
   __syncwarp();
   if (nsub > 0) {
-    const int K = words_k(n), RS = K + 1;
+    const int K = words_k(n), RS = rec_stride(K);
     uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
     init_records(rec, K, nsub);
     flat_rows(
@@ -1261,7 +1280,7 @@ __device__ void t1_sparse_push(Warp& W, const T1& t, int x, int level, int kept,
   if (ism && kept > 1 && ncand > 0) {
     // Destination: an export slot when idle warps want work and the child is
     // big enough by GMBE's split test, else this warp's scratch.
-    const int K = words_k(n), RS = K + 1;
+    const int K = words_k(n), RS = rec_stride(K);
     int slot = -1;
     if (slot_fits(W, ncand, K) && should_export(W, ncand - nqc, n, W.p.eager_share != 0)) {
       slot = lane == 0 ? slot_alloc_for(W, ncand, K) : 0;
@@ -2366,7 +2385,7 @@ __device__ void run_task(Warp& W, const Task& t) {
       if (W.p.emit)
         for (int l = lane; l < nL; l += 32) lid[l] = L[l];
       for (int i = lane; i < nC; i += 32) subkey[i] = g.vkey[cv[i]];
-      const int K = words_k(nL), RS = K + 1;
+      const int K = words_k(nL), RS = rec_stride(K);
       uint32_t* rec = reinterpret_cast<uint32_t*>(W.A(W.sl.masks));
       init_records(rec, K, nC);
       flat_rows(
