@@ -283,6 +283,21 @@ def test_server_needs_a_device(gm):
     assert ei.value.name == "MBE_ERR_CUDA"
 
 
+def test_new_entry_points_check_arguments_before_any_device_call(gm):
+    # mbe_measure_l2_read refuses sizes outside 1-96 MiB and passes outside
+    # 1-1000; mbe_server_set_emit refuses a null server or callback.  Both
+    # before touching a device.
+    for nbytes, passes in ((1 << 10, 10), (1 << 30, 10), (32 << 20, 0), (32 << 20, 5000)):
+        with pytest.raises(gm.MBEError) as ei:
+            gm.measure_l2_read(0, nbytes, passes)
+        assert ei.value.name == "MBE_ERR_INVALID"
+    import ctypes as C
+    lib = C.CDLL(gm.LIB_PATH)
+    lib.mbe_server_set_emit.restype = C.c_int
+    lib.mbe_server_set_emit.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    assert lib.mbe_server_set_emit(None, 0, None, None) == -1  # MBE_ERR_INVALID
+
+
 def test_graph_writer_matches_reference_converter(gm, tmp_path):
     # The edge-pair .graph file the CPU peers read.  Where the reference's own
     # converter (preprocess/adj_to_graph.cpp) is built into oracle/_ref, both
