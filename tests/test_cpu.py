@@ -298,6 +298,20 @@ def test_new_entry_points_check_arguments_before_any_device_call(gm):
     assert lib.mbe_server_set_emit(None, 0, None, None) == -1  # MBE_ERR_INVALID
 
 
+def test_large_shard_pins_agree_with_the_reference():
+    # tests/golden/pin_large_shards_reference.py ran the reference's own
+    # MbeaFinderBitset on every root of the pinned large-graph shards; its
+    # counts must equal the oracle's (the reference reports counts only).
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "large_shards.json")) as f:
+        d = json.load(f)
+    pinned = [sh for sh in d["shards"] if "reference_count" in sh]
+    assert pinned, "no shard carries the reference's count"
+    for sh in pinned:
+        assert sh["reference_count"] == sh["count"], sh["shard_index"]
+
+
 def test_graph_writer_matches_reference_converter(gm, tmp_path):
     # The edge-pair .graph file the CPU peers read.  Where the reference's own
     # converter (preprocess/adj_to_graph.cpp) is built into oracle/_ref, both
