@@ -312,6 +312,18 @@ def test_large_shard_pins_agree_with_the_reference():
         assert sh["reference_count"] == sh["count"], sh["shard_index"]
 
 
+def test_batch_fixture_agrees_with_the_reference():
+    # tests/golden/pin_batch_reference.py ran the reference's own
+    # MbeaFinderBitset on all 4,096 graphs of the batched workload; every
+    # count must equal the oracle's.
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "batch_oracle.json")) as f:
+        d = json.load(f)
+    assert len(d["reference_count"]) == d["n"] == len(d["count"])
+    assert d["reference_count"] == d["count"]
+
+
 def test_graph_writer_matches_reference_converter(gm, tmp_path):
     # The edge-pair .graph file the CPU peers read.  Where the reference's own
     # converter (preprocess/adj_to_graph.cpp) is built into oracle/_ref, both
